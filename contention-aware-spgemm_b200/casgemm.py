@@ -1,0 +1,333 @@
+"""Python binding of the casgemm C ABI (include/casgemm.h, include/casgemm_data.h).
+
+A thin ctypes layer over libcasgemm.so: no computation happens here.  The
+product path is the CUDA library; if it is missing, :func:`load` raises.
+
+Mirrors the reference's call surface (fukien/contention-aware-spgemm): one
+call per accumulator — ``hash``, ``hsersc``, ``hybacc`` for
+ams_hashspgemm / ams_hserscspgemm / ams_hybaccspgemm — returning C with the
+phase times of the reference's runtime_t (src/mm/mm_utils.h:48-54).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcasgemm.so")
+
+ACCUM = {"hash": 0, "hsersc": 1, "hybacc": 2}
+VAL_F64, VAL_I32 = 0, 1
+STATUS = {
+    0: "CAS_OK", 1: "CAS_ERR_BAD_INPUT", 2: "CAS_ERR_OOM", 3: "CAS_ERR_CUDA",
+    4: "CAS_ERR_DEVICE", 5: "CAS_ERR_TIMEOUT", 6: "CAS_ERR_ABORTED", 7: "CAS_ERR_REJECTED",
+}
+SYMB_BINS = ["zero", "tiny", "h512", "h2k", "h8k", "h32k", "dense"]
+NUMC_BINS = ["zero", "tiny", "esc1k", "esc2k", "esc4k", "esc8k", "hash256", "hash1k", "hash4k", "dense"]
+
+
+class CasCsr(ctypes.Structure):
+    _fields_ = [
+        ("num_row", ctypes.c_int64), ("num_col", ctypes.c_int64), ("num_nnz", ctypes.c_int64),
+        ("row_ptrs", ctypes.c_void_p), ("cols", ctypes.c_void_p), ("rats", ctypes.c_void_p),
+        ("col_bytes", ctypes.c_int32), ("val_type", ctypes.c_int32),
+        ("on_device", ctypes.c_int32), ("owned", ctypes.c_int32),
+    ]
+
+
+class CasRuntime(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("init_time", "symb_time", "mgmt_time", "numc_time", "total_time")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class CasStats(ctypes.Structure):
+    _fields_ = [
+        ("flop", ctypes.c_int64), ("max_row_flp", ctypes.c_int64), ("nnz_c", ctypes.c_int64),
+        ("symb_bin_rows", ctypes.c_int64 * 7), ("numc_bin_rows", ctypes.c_int64 * 10),
+        ("kernel_launches", ctypes.c_int64), ("h2d_bytes", ctypes.c_double), ("d2h_bytes", ctypes.c_double),
+    ]
+
+
+class CasError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libcasgemm.so (raises FileNotFoundError when it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with `make -C {HERE}` (or __graft_entry__.build())")
+    lib = ctypes.CDLL(path)
+    P, I64, I32, D = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_double
+    sig = {
+        "cas_create": (I32, [ctypes.c_int, ctypes.POINTER(P)]),
+        "cas_destroy": (None, [P]),
+        "cas_set_stream": (I32, [P, P]),
+        "cas_set_acc_thres": (I32, [P, D]),
+        "cas_last_error": (ctypes.c_char_p, [P]),
+        "cas_get_stats": (I32, [P, ctypes.POINTER(CasStats)]),
+        "cas_spgemm": (I32, [P, I32, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr),
+                             ctypes.POINTER(CasRuntime)]),
+        "cas_csr_free": (I32, [P, ctypes.POINTER(CasCsr)]),
+        "cas_flp_populate": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), P]),
+        "cas_scan": (I32, [P, P, P, I64]),
+        "cas_hash_symb": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), P, P]),
+        "cas_hash_numc": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), P, ctypes.POINTER(CasCsr)]),
+        "cas_hsersc_numc": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), P, ctypes.POINTER(CasCsr)]),
+        "cas_hybacc_numc": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), P, ctypes.POINTER(CasCsr)]),
+        "cas_gen_rmat": (I32, [ctypes.c_int, ctypes.c_int, D, D, D, ctypes.c_uint64, P, P]),
+        "cas_zipf_row_degrees": (D, [I64, I64, D, I64, P]),
+        "cas_gen_zipf": (I64, [I64, I64, I64, D, I64, D, D, ctypes.c_uint64, P, P]),
+        "cas_gen_int_values": (None, [I64, I32, I32, ctypes.c_uint64, P]),
+        "cas_csr_transpose_host": (I32, [I64, I64, P, P, P, ctypes.c_int, P, P, P]),
+        "cas_intprod_host": (I64, [I64, P, P, P]),
+        "cas_mtx_read": (I64, [ctypes.c_char_p, ctypes.POINTER(I64), ctypes.POINTER(I64), P, P, P]),
+        "cas_mtx_write": (I32, [ctypes.c_char_p, I64, I64, P, P, ctypes.c_int]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a: Optional[np.ndarray]) -> Optional[int]:
+    return None if a is None else a.ctypes.data
+
+
+# ------------------------------------------------------------------ matrices
+@dataclass
+class Csr:
+    """Host CSR: int64 row pointers, int32 columns, float64 or int32 values."""
+    num_row: int
+    num_col: int
+    row_ptrs: np.ndarray
+    cols: np.ndarray
+    vals: np.ndarray
+
+    @property
+    def nnz(self) -> int:
+        return int(self.row_ptrs[-1]) if len(self.row_ptrs) else 0
+
+    @property
+    def val_type(self) -> int:
+        return VAL_I32 if self.vals.dtype == np.int32 else VAL_F64
+
+    def as_cas(self) -> CasCsr:
+        rp = np.ascontiguousarray(self.row_ptrs, dtype=np.int64)
+        cols = np.ascontiguousarray(self.cols)
+        vals = np.ascontiguousarray(self.vals)
+        self._keep = (rp, cols, vals)
+        return CasCsr(self.num_row, self.num_col, self.nnz, rp.ctypes.data, cols.ctypes.data, vals.ctypes.data,
+                      cols.dtype.itemsize, self.val_type, 0, 0)
+
+    def transpose(self) -> "Csr":
+        return transpose(self)
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        return sp.csr_matrix((self.vals, self.cols, self.row_ptrs), shape=(self.num_row, self.num_col))
+
+
+@dataclass
+class Result:
+    """C = A*B on the host, with the call's phase times and counters."""
+    csr: Csr
+    runtime: dict
+    stats: dict = field(default_factory=dict)
+
+
+class DeviceCsr:
+    """A device CSR described by raw pointers (e.g. torch CUDA tensors' data_ptr)."""
+
+    def __init__(self, num_row, num_col, nnz, row_ptrs_ptr, cols_ptr, vals_ptr, val_type=VAL_F64, keep=None):
+        self.c = CasCsr(num_row, num_col, nnz, row_ptrs_ptr, cols_ptr, vals_ptr, 4, val_type, 1, 0)
+        self._keep = keep
+
+
+class Context:
+    """A casgemm context on one device (cas_create / cas_destroy)."""
+
+    def __init__(self, device: int = 0, acc_thres: float = 2.0):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        st = self.lib.cas_create(device, ctypes.byref(h))
+        if st != 0:
+            raise CasError(st, "cas_create failed")
+        self.h = h
+        self.set_acc_thres(acc_thres)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cas_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st != 0:
+            raise CasError(st, self.lib.cas_last_error(self.h).decode())
+
+    def set_acc_thres(self, thres: float):
+        self._check(self.lib.cas_set_acc_thres(self.h, float(thres)))
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        self._check(self.lib.cas_set_stream(self.h, stream_ptr))
+
+    def stats(self) -> dict:
+        s = CasStats()
+        self._check(self.lib.cas_get_stats(self.h, ctypes.byref(s)))
+        return {
+            "flop": s.flop, "max_row_flp": s.max_row_flp, "nnz_c": s.nnz_c,
+            "symb_bins": dict(zip(SYMB_BINS, list(s.symb_bin_rows))),
+            "numc_bins": dict(zip(NUMC_BINS, list(s.numc_bin_rows))),
+            "kernel_launches": s.kernel_launches, "h2d_bytes": s.h2d_bytes, "d2h_bytes": s.d2h_bytes,
+        }
+
+    def spgemm(self, A, B, accum: str = "hybacc", col_bytes: int = 4) -> Result:
+        """C = A*B for host CSR inputs (Csr or CasCsr), returned on the host."""
+        ca = A.as_cas() if isinstance(A, Csr) else A
+        cb = B.as_cas() if isinstance(B, Csr) else B
+        cc = CasCsr()
+        cc.on_device = 0
+        cc.col_bytes = col_bytes
+        rt = CasRuntime()
+        self._check(self.lib.cas_spgemm(self.h, ACCUM[accum], ctypes.byref(ca), ctypes.byref(cb), ctypes.byref(cc),
+                                        ctypes.byref(rt)))
+        try:
+            m, nnz = cc.num_row, cc.num_nnz
+            rp = np.ctypeslib.as_array(ctypes.cast(cc.row_ptrs, ctypes.POINTER(ctypes.c_int64)), (m + 1,)).copy()
+            ctype = ctypes.c_int32 if cc.col_bytes == 4 else ctypes.c_int64
+            vtype = ctypes.c_double if cc.val_type == VAL_F64 else ctypes.c_int64
+            if nnz > 0:
+                cols = np.ctypeslib.as_array(ctypes.cast(cc.cols, ctypes.POINTER(ctype)), (nnz,)).copy()
+                vals = np.ctypeslib.as_array(ctypes.cast(cc.rats, ctypes.POINTER(vtype)), (nnz,)).copy()
+            else:
+                cols = np.zeros(0, np.int32 if cc.col_bytes == 4 else np.int64)
+                vals = np.zeros(0, np.float64 if cc.val_type == VAL_F64 else np.int64)
+            C = Csr(cc.num_row, cc.num_col, rp, cols, vals)
+        finally:
+            self.lib.cas_csr_free(self.h, ctypes.byref(cc))
+        return Result(C, rt.as_dict(), self.stats())
+
+    def spgemm_device(self, A: DeviceCsr, B: DeviceCsr, accum: str = "hybacc"):
+        """C = A*B for device inputs; returns (CasCsr owned by the library, runtime).
+
+        Release the result with :meth:`free`."""
+        cc = CasCsr()
+        cc.on_device = 1
+        rt = CasRuntime()
+        self._check(self.lib.cas_spgemm(self.h, ACCUM[accum], ctypes.byref(A.c), ctypes.byref(B.c),
+                                        ctypes.byref(cc), ctypes.byref(rt)))
+        return cc, rt.as_dict()
+
+    def free(self, cc: CasCsr):
+        self._check(self.lib.cas_csr_free(self.h, ctypes.byref(cc)))
+
+
+# ---------------------------------------------------------------- data layer
+def gen_rmat(scale: int, edge_factor: int, a: float, b: float, c: float, seed: int) -> Csr:
+    """Symmetrised loop-free duplicate-free R-MAT graph (values 1.0)."""
+    lib = load()
+    n = 1 << scale
+    nnz = 2 * edge_factor * n
+    rp = np.empty(n + 1, np.int64)
+    cols = np.empty(nnz, np.int32)
+    st = lib.cas_gen_rmat(scale, edge_factor, a, b, c, seed, _ptr(rp), _ptr(cols))
+    if st != 0:
+        raise ValueError(f"cas_gen_rmat failed for scale={scale} ef={edge_factor}")
+    return Csr(n, n, rp, cols, np.ones(nnz, np.float64))
+
+
+def gen_g500(scale: int, edge_factor: int, seed: int) -> Csr:
+    return gen_rmat(scale, edge_factor, 0.57, 0.19, 0.19, seed)
+
+
+def gen_er(scale: int, edge_factor: int, seed: int) -> Csr:
+    return gen_rmat(scale, edge_factor, 0.25, 0.25, 0.25, seed)
+
+
+def gen_zipf(num_row: int, num_col: int, amax: int, target_nnz: int, seed: int,
+             row_s: float = 1.2, col_s: float = 1.4, col_q: float = 1000.0) -> Csr:
+    lib = load()
+    rp = np.empty(num_row + 1, np.int64)
+    nnz = lib.cas_gen_zipf(num_row, num_col, amax, row_s, target_nnz, col_s, col_q, seed, _ptr(rp), None)
+    if nnz < 0:
+        raise ValueError("cas_gen_zipf failed")
+    cols = np.empty(nnz, np.int32)
+    nnz2 = lib.cas_gen_zipf(num_row, num_col, amax, row_s, target_nnz, col_s, col_q, seed, _ptr(rp), _ptr(cols))
+    if nnz2 != nnz:
+        raise ValueError("cas_gen_zipf failed")
+    return Csr(num_row, num_col, rp, cols, np.ones(nnz, np.float64))
+
+
+def int_values(nnz: int, seed: int, lo: int = 1, hi: int = 8) -> np.ndarray:
+    v = np.empty(nnz, np.int32)
+    load().cas_gen_int_values(nnz, lo, hi, seed, _ptr(v))
+    return v
+
+
+def transpose(A: Csr) -> Csr:
+    lib = load()
+    rp = np.empty(A.num_col + 1, np.int64)
+    cols = np.empty(A.nnz, np.int32)
+    vals = np.empty(A.nnz, A.vals.dtype)
+    cols_in = np.ascontiguousarray(A.cols, dtype=np.int32)
+    st = lib.cas_csr_transpose_host(A.num_row, A.num_col, _ptr(np.ascontiguousarray(A.row_ptrs, np.int64)),
+                                    _ptr(cols_in), _ptr(np.ascontiguousarray(A.vals)), A.vals.dtype.itemsize,
+                                    _ptr(rp), _ptr(cols), _ptr(vals))
+    if st != 0:
+        raise ValueError("transpose failed")
+    return Csr(A.num_col, A.num_row, rp, cols, vals)
+
+
+def intprod(A: Csr, B: Csr) -> int:
+    """Intermediate products of A*B (the reference's flop_cnt)."""
+    return int(load().cas_intprod_host(A.num_row, _ptr(np.ascontiguousarray(A.row_ptrs, np.int64)),
+                                       _ptr(np.ascontiguousarray(A.cols, np.int32)),
+                                       _ptr(np.ascontiguousarray(B.row_ptrs, np.int64))))
+
+
+def mtx_read(path: str) -> Csr:
+    """MatrixMarket -> CSR with the reference loader's semantics (values forced to 1.0)."""
+    lib = load()
+    nr, nc = ctypes.c_int64(), ctypes.c_int64()
+    nnz = lib.cas_mtx_read(path.encode(), ctypes.byref(nr), ctypes.byref(nc), None, None, None)
+    if nnz < 0:
+        raise ValueError(f"cannot read {path}")
+    rp = np.empty(nr.value + 1, np.int64)
+    cols = np.empty(nnz, np.int32)
+    vals = np.empty(nnz, np.float64)
+    if lib.cas_mtx_read(path.encode(), ctypes.byref(nr), ctypes.byref(nc), _ptr(rp), _ptr(cols), _ptr(vals)) != nnz:
+        raise ValueError(f"cannot read {path}")
+    return Csr(nr.value, nc.value, rp, cols, vals)
+
+
+def mtx_write(path: str, A: Csr, symmetric: bool):
+    if load().cas_mtx_write(path.encode(), A.num_row, A.num_col, _ptr(np.ascontiguousarray(A.row_ptrs, np.int64)),
+                            _ptr(np.ascontiguousarray(A.cols, np.int32)), int(symmetric)) != 0:
+        raise ValueError(f"cannot write {path}")

@@ -1,0 +1,843 @@
+// casgemm C ABI and host orchestration (declarations in include/casgemm.h).
+//
+// One call of cas_spgemm runs the four phases of the reference's drivers
+// (src/ams_hybaccspgemm.c:36-215) on the context's stream:
+//   INIT  input check, k_flp (row products, totals, symbolic bin histogram),
+//         symbolic bin lists
+//   SYMB  symbolic kernels per bin (bins run concurrently on auxiliary
+//         streams), scan of the counts into C's row pointers
+//   MGMT  allocation of C, numeric bin lists
+//   NUMC  numeric kernels per bin
+// Each phase boundary is a CUDA event; the phase times are what cas_runtime
+// reports, like the reference's runtime_t.  The host waits three times per
+// call, each to size the next phase (bin counts, nnz(C)).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "casgemm.h"
+#include "cas_kernels.cu"
+
+namespace {
+
+constexpr int kAux = 4;          // auxiliary streams for concurrent bins
+constexpr int kCountSlots = 64;  // device/pinned counter block
+
+// Layout of the counter block (unsigned long long slots).
+constexpr int kSlotSymb = 0;     // [0, 7)   symbolic bin counts
+constexpr int kSlotNumc = 8;     // [8, 18)  numeric bin counts
+constexpr int kSlotTotals = 20;  // [20]    products, [21] max row products
+constexpr int kSlotCursor = 24;  // [24, 40) bin cursors
+constexpr int kSlotNnz = 44;     // [44]    nnz(C) from the scan
+constexpr int kSlotCheck = 48;   // [48]    input check flags
+
+}  // namespace
+
+struct cas_ctx {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaStream_t aux[kAux] = {};
+  cudaEvent_t ev_fork = nullptr;
+  cudaEvent_t ev_join[kAux] = {};
+  cudaEvent_t ev_phase[5] = {};
+  double acc_thres = 2.0;
+  std::string err;
+  cas_stats stats{};
+  int64_t launches = 0;
+  cas::DevStatus* d_status = nullptr;
+  unsigned long long* d_counts = nullptr;
+  unsigned long long* h_counts = nullptr;  // pinned mirror
+  cas::DevStatus* h_status = nullptr;      // pinned mirror
+};
+
+namespace {
+
+using cas::Csr;
+
+cas_status set_err(cas_ctx* ctx, cas_status st, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->err = buf;
+  return st;
+}
+
+#define CAS_CUDA(ctx, call)                                                                  \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess) {                                                                 \
+      return set_err(ctx, e_ == cudaErrorMemoryAllocation ? CAS_ERR_OOM : CAS_ERR_CUDA,      \
+                     "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    }                                                                                        \
+  } while (0)
+
+#define CAS_TRY(x)                      \
+  do {                                  \
+    cas_status s_ = (x);                \
+    if (s_ != CAS_OK) return s_;        \
+  } while (0)
+
+cas_status check_launch(cas_ctx* ctx, const char* what) {
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(ctx, CAS_ERR_CUDA, "launch of %s failed: %s", what, cudaGetErrorString(e));
+  return CAS_OK;
+}
+
+const char* dev_err_name(int code) {
+  switch (code) {
+    case cas::kDevRowOverflow: return "a row produced more entries than its symbolic count";
+    case cas::kDevRowUnderflow: return "a row produced fewer entries than its symbolic count";
+    case cas::kDevCapacity: return "a row exceeded the shared-memory capacity of its kernel";
+    case cas::kDevTableFull: return "a shared-memory hash table ran out of slots";
+    case cas::kDevBadIndex: return "a column index is outside the matrix";
+    default: return "unknown device error";
+  }
+}
+
+cas_status check_status(cas_ctx* ctx) {
+  CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(cas::DevStatus), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ctx->h_status->err != 0) {
+    return set_err(ctx, CAS_ERR_DEVICE, "device check failed in kernel %d at row %lld: %s", ctx->h_status->kernel,
+                   (long long)ctx->h_status->row, dev_err_name(ctx->h_status->err));
+  }
+  return CAS_OK;
+}
+
+template <typename K>
+cas_status allow_smem(cas_ctx* ctx, K kernel, size_t bytes) {
+  CAS_CUDA(ctx, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return CAS_OK;
+}
+
+// ------------------------------------------------ kernel shapes and memory
+template <int BLOCK, int TBITS>
+constexpr size_t smem_symb_hash() { return (size_t(1) << TBITS) * 4 + sizeof(cas::Stage<double>); }
+template <int BLOCK>
+constexpr size_t smem_symb_dense() { return size_t(cas::kDenseChunkBits / 32) * 4 + sizeof(cas::Stage<double>); }
+template <int BLOCK, int CAP, typename VIn>
+constexpr size_t smem_numc_esc() {
+  return size_t(CAP) * 16 + size_t(CAP) * sizeof(typename cas::Acc<VIn>::T) + sizeof(cas::SortScratch<BLOCK>) +
+         sizeof(cas::Stage<VIn>);
+}
+template <int BLOCK, int TBITS, typename VIn>
+constexpr size_t smem_numc_hash() {
+  return (size_t(1) << TBITS) * (4 + sizeof(typename cas::Acc<VIn>::T)) + (size_t(1) << (TBITS - 1)) * 8 +
+         sizeof(cas::SortScratch<BLOCK>) + sizeof(cas::Stage<VIn>);
+}
+template <int BLOCK, typename VIn>
+constexpr size_t smem_numc_dense() {
+  return size_t(cas::kDenseChunkCols) * sizeof(typename cas::Acc<VIn>::T) + size_t(cas::kDenseChunkCols / 32) * 4 +
+         sizeof(cas::Stage<VIn>);
+}
+
+template <typename VIn>
+cas_status setup_numc_kernels(cas_ctx* ctx) {
+  using namespace cas;
+  CAS_TRY(allow_smem(ctx, k_numc_esc<256, 1024, VIn>, smem_numc_esc<256, 1024, VIn>()));
+  CAS_TRY(allow_smem(ctx, k_numc_esc<256, 2048, VIn>, smem_numc_esc<256, 2048, VIn>()));
+  CAS_TRY(allow_smem(ctx, k_numc_esc<512, 4096, VIn>, smem_numc_esc<512, 4096, VIn>()));
+  CAS_TRY(allow_smem(ctx, k_numc_esc<1024, 8192, VIn>, smem_numc_esc<1024, 8192, VIn>()));
+  CAS_TRY(allow_smem(ctx, k_numc_hash<256, 9, VIn>, smem_numc_hash<256, 9, VIn>()));
+  CAS_TRY(allow_smem(ctx, k_numc_hash<256, 11, VIn>, smem_numc_hash<256, 11, VIn>()));
+  CAS_TRY(allow_smem(ctx, k_numc_hash<512, 13, VIn>, smem_numc_hash<512, 13, VIn>()));
+  CAS_TRY(allow_smem(ctx, k_numc_dense<1024, VIn>, smem_numc_dense<1024, VIn>()));
+  return CAS_OK;
+}
+
+cas_status setup_kernels(cas_ctx* ctx) {
+  using namespace cas;
+  CAS_TRY(allow_smem(ctx, k_symb_hash<128, 9>, smem_symb_hash<128, 9>()));
+  CAS_TRY(allow_smem(ctx, k_symb_hash<256, 11>, smem_symb_hash<256, 11>()));
+  CAS_TRY(allow_smem(ctx, k_symb_hash<512, 13>, smem_symb_hash<512, 13>()));
+  CAS_TRY(allow_smem(ctx, k_symb_hash<1024, 15>, smem_symb_hash<1024, 15>()));
+  CAS_TRY(allow_smem(ctx, k_symb_dense<1024>, smem_symb_dense<1024>()));
+  CAS_TRY(setup_numc_kernels<double>(ctx));
+  CAS_TRY(setup_numc_kernels<int32_t>(ctx));
+  return CAS_OK;
+}
+
+int grid_for(int64_t items, int block, int cap) {
+  int64_t g = (items + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+// ------------------------------------------------------- device matrices
+struct DevMat {
+  Csr csr{};
+  int64_t nnz = 0;
+  int vt = CAS_VAL_F64;
+  std::vector<void*> owned;  // temporaries allocated for a host input
+};
+
+cas_status free_owned(cas_ctx* ctx, DevMat& m) {
+  for (void* p : m.owned) CAS_CUDA(ctx, cudaFreeAsync(p, ctx->stream));
+  m.owned.clear();
+  return CAS_OK;
+}
+
+cas_status dev_alloc(cas_ctx* ctx, void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMallocAsync(p, bytes, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, e == cudaErrorMemoryAllocation ? CAS_ERR_OOM : CAS_ERR_CUDA,
+                   "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+  }
+  return CAS_OK;
+}
+
+cas_status basic_checks(cas_ctx* ctx, const cas_csr* M, const char* name) {
+  if (!M) return set_err(ctx, CAS_ERR_BAD_INPUT, "%s is NULL", name);
+  if (M->num_row < 0 || M->num_col < 0 || M->num_nnz < 0 || M->num_row > INT32_MAX || M->num_col > INT32_MAX)
+    return set_err(ctx, CAS_ERR_BAD_INPUT, "%s has an invalid shape", name);
+  if (!M->row_ptrs || (M->num_nnz > 0 && (!M->cols || !M->rats)))
+    return set_err(ctx, CAS_ERR_BAD_INPUT, "%s has NULL arrays", name);
+  if (M->val_type != CAS_VAL_F64 && M->val_type != CAS_VAL_I32)
+    return set_err(ctx, CAS_ERR_BAD_INPUT, "%s has an unknown value type", name);
+  if (M->on_device ? M->col_bytes != 4 : (M->col_bytes != 4 && M->col_bytes != 8))
+    return set_err(ctx, CAS_ERR_BAD_INPUT, "%s has column width %d", name, M->col_bytes);
+  return CAS_OK;
+}
+
+cas_status to_device(cas_ctx* ctx, const cas_csr* M, DevMat& out, double& h2d) {
+  out.csr.nrow = M->num_row;
+  out.csr.ncol = M->num_col;
+  out.nnz = M->num_nnz;
+  out.vt = M->val_type;
+  const size_t vbytes = M->val_type == CAS_VAL_F64 ? 8 : 4;
+  if (M->on_device) {
+    out.csr.rp = M->row_ptrs;
+    out.csr.col = static_cast<const int32_t*>(M->cols);
+    out.csr.val = M->rats;
+    return CAS_OK;
+  }
+  if (M->row_ptrs[0] != 0 || M->row_ptrs[M->num_row] != M->num_nnz)
+    return set_err(ctx, CAS_ERR_BAD_INPUT, "row pointers do not span [0, num_nnz]");
+  void *rp, *col, *val;
+  CAS_TRY(dev_alloc(ctx, &rp, sizeof(int64_t) * (M->num_row + 1)));
+  out.owned.push_back(rp);
+  CAS_TRY(dev_alloc(ctx, &col, sizeof(int32_t) * M->num_nnz));
+  out.owned.push_back(col);
+  CAS_TRY(dev_alloc(ctx, &val, vbytes * M->num_nnz));
+  out.owned.push_back(val);
+  CAS_CUDA(ctx, cudaMemcpyAsync(rp, M->row_ptrs, sizeof(int64_t) * (M->num_row + 1), cudaMemcpyHostToDevice, ctx->stream));
+  if (M->col_bytes == 4) {
+    CAS_CUDA(ctx, cudaMemcpyAsync(col, M->cols, sizeof(int32_t) * M->num_nnz, cudaMemcpyHostToDevice, ctx->stream));
+    h2d += sizeof(int32_t) * (double)M->num_nnz;
+  } else {
+    // the reference's int64 columns: narrowed on the host
+    std::vector<int32_t> tmp((size_t)M->num_nnz);
+    const int64_t* c64 = static_cast<const int64_t*>(M->cols);
+    for (int64_t i = 0; i < M->num_nnz; ++i) {
+      if (c64[i] < 0 || c64[i] > INT32_MAX) return set_err(ctx, CAS_ERR_BAD_INPUT, "column index out of int32 range");
+      tmp[(size_t)i] = (int32_t)c64[i];
+    }
+    CAS_CUDA(ctx, cudaMemcpyAsync(col, tmp.data(), sizeof(int32_t) * M->num_nnz, cudaMemcpyHostToDevice, ctx->stream));
+    CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    h2d += sizeof(int64_t) * (double)M->num_nnz;
+  }
+  CAS_CUDA(ctx, cudaMemcpyAsync(val, M->rats, vbytes * M->num_nnz, cudaMemcpyHostToDevice, ctx->stream));
+  h2d += sizeof(int64_t) * (double)(M->num_row + 1) + vbytes * (double)M->num_nnz;
+  out.csr.rp = static_cast<const int64_t*>(rp);
+  out.csr.col = static_cast<const int32_t*>(col);
+  out.csr.val = val;
+  return CAS_OK;
+}
+
+}  // namespace
+
+// ============================================================ input check
+namespace cas {
+// One warp per row: row pointers non-decreasing and within [0, nnz], column
+// indices in [0, ncol); flags[1] is set when some row is not sorted.
+__global__ void k_check_csr(Csr M, int64_t nnz, unsigned long long* flags) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < M.nrow; r += nw) {
+    const int64_t s = M.rp[r], e = M.rp[r + 1];
+    if (s < 0 || e < s || e > nnz) {
+      if (lane == 0) atomicOr(&flags[0], 1ull);
+      continue;
+    }
+    bool bad = false, unsorted = false;
+    for (int64_t j = s + lane; j < e; j += 32) {
+      const int32_t c = M.col[j];
+      bad |= (uint64_t)c >= (uint64_t)M.ncol;
+      if (j + 1 < e) unsorted |= M.col[j + 1] < c;
+    }
+    if (__any_sync(kFull, bad) && lane == 0) atomicOr(&flags[0], 1ull);
+    if (__any_sync(kFull, unsorted) && lane == 0) atomicOr(&flags[1], 1ull);
+  }
+}
+}  // namespace cas
+
+namespace {
+
+struct Call {
+  DevMat A, B;
+  int64_t m = 0, ncol = 0;
+  int vt = CAS_VAL_F64;
+  int64_t* row_flp = nullptr;
+  int64_t* row_nz = nullptr;
+  int32_t* rows = nullptr;
+  int64_t* partial = nullptr;
+  int64_t nparts = 0;
+  bool b_sorted = true;
+  int64_t symb_count[cas::kSymbBins] = {};
+  int64_t numc_count[cas::kNumcBins] = {};
+  int64_t flop = 0, max_flp = 0;
+};
+
+cas_status fork(cas_ctx* ctx) {
+  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
+  for (int i = 0; i < kAux; ++i) CAS_CUDA(ctx, cudaStreamWaitEvent(ctx->aux[i], ctx->ev_fork, 0));
+  return CAS_OK;
+}
+cas_status join(cas_ctx* ctx) {
+  for (int i = 0; i < kAux; ++i) {
+    CAS_CUDA(ctx, cudaEventRecord(ctx->ev_join[i], ctx->aux[i]));
+    CAS_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_join[i], 0));
+  }
+  return CAS_OK;
+}
+
+cas_status scratch_alloc(cas_ctx* ctx, Call& c) {
+  CAS_TRY(dev_alloc(ctx, (void**)&c.row_flp, sizeof(int64_t) * (c.m + 1)));
+  CAS_TRY(dev_alloc(ctx, (void**)&c.row_nz, sizeof(int64_t) * (c.m + 1)));
+  CAS_TRY(dev_alloc(ctx, (void**)&c.rows, sizeof(int32_t) * (c.m + 1)));
+  c.nparts = (c.m + 1 + cas::kScanTile - 1) / cas::kScanTile;
+  CAS_TRY(dev_alloc(ctx, (void**)&c.partial, sizeof(int64_t) * (c.nparts + 1)));
+  return CAS_OK;
+}
+
+cas_status scratch_free(cas_ctx* ctx, Call& c) {
+  void* ps[] = {c.row_flp, c.row_nz, c.rows, c.partial};
+  for (void* p : ps)
+    if (p) CAS_CUDA(ctx, cudaFreeAsync(p, ctx->stream));
+  c.row_flp = c.row_nz = nullptr;
+  c.rows = nullptr;
+  c.partial = nullptr;
+  return CAS_OK;
+}
+
+// exclusive scan of in[0..n-1) into out[0..n), total of in into counter slot
+cas_status launch_scan(cas_ctx* ctx, int64_t* out, const int64_t* in, int64_t n, int64_t* partial,
+                       int64_t* total_out) {
+  using namespace cas;
+  if (n <= 0) return CAS_OK;
+  const int64_t n_in = n - 1;
+  const int64_t nparts = (n + kScanTile - 1) / kScanTile;
+  k_scan_partials<<<(unsigned)nparts, kScanBlock, 0, ctx->stream>>>(in, n_in, partial);
+  CAS_TRY(check_launch(ctx, "k_scan_partials"));
+  k_scan_top<<<1, kScanBlock, 0, ctx->stream>>>(partial, nparts, total_out);
+  CAS_TRY(check_launch(ctx, "k_scan_top"));
+  k_scan_apply<<<(unsigned)nparts, kScanBlock, 0, ctx->stream>>>(in, n_in, partial, out, n);
+  CAS_TRY(check_launch(ctx, "k_scan_apply"));
+  return CAS_OK;
+}
+
+// ------------------------------------------------------------------ INIT
+cas_status phase_init(cas_ctx* ctx, Call& c, bool validate) {
+  using namespace cas;
+  CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_counts, 0, sizeof(unsigned long long) * kCountSlots, ctx->stream));
+  CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(DevStatus), ctx->stream));
+  CAS_TRY(scratch_alloc(ctx, c));
+  if (validate) {
+    const int g = grid_for(std::max<int64_t>(c.A.csr.nrow, c.B.csr.nrow) * 32, 256, ctx->sm_count * 16);
+    Csr a = c.A.csr;
+    a.ncol = c.B.csr.nrow;  // A's columns index B's rows
+    k_check_csr<<<g, 256, 0, ctx->stream>>>(a, c.A.nnz, ctx->d_counts + kSlotCheck);
+    CAS_TRY(check_launch(ctx, "k_check_csr"));
+    k_check_csr<<<g, 256, 0, ctx->stream>>>(c.B.csr, c.B.nnz, ctx->d_counts + kSlotCheck + 2);
+    CAS_TRY(check_launch(ctx, "k_check_csr"));
+  }
+  if (c.m > 0) {
+    k_flp<256><<<grid_for(c.m * 32, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+        c.A.csr, c.B.csr, c.ncol, c.row_flp, ctx->d_counts + kSlotTotals, ctx->d_counts + kSlotSymb, ctx->d_status);
+    CAS_TRY(check_launch(ctx, "k_flp"));
+  }
+  CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, sizeof(unsigned long long) * kCountSlots,
+                                cudaMemcpyDeviceToHost, ctx->stream));
+  CAS_TRY(check_status(ctx));  // synchronises
+  if (validate) {
+    if (ctx->h_counts[kSlotCheck] || ctx->h_counts[kSlotCheck + 2])
+      return set_err(ctx, CAS_ERR_BAD_INPUT, "invalid CSR input: row pointers or column indices out of range");
+    c.b_sorted = ctx->h_counts[kSlotCheck + 3] == 0;
+  } else {
+    c.b_sorted = false;
+  }
+  c.flop = (int64_t)ctx->h_counts[kSlotTotals];
+  c.max_flp = (int64_t)ctx->h_counts[kSlotTotals + 1];
+  unsigned long long* cur = ctx->h_counts + kSlotCursor;
+  unsigned long long off = 0;
+  for (int b = 0; b < kSymbBins; ++b) {
+    c.symb_count[b] = (int64_t)ctx->h_counts[kSlotSymb + b];
+    cur[b] = off;
+    off += ctx->h_counts[kSlotSymb + b];
+  }
+  if (c.m > 0) {
+    CAS_CUDA(ctx, cudaMemcpyAsync(ctx->d_counts + kSlotCursor, cur, sizeof(unsigned long long) * kSymbBins,
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    k_bin_scatter_symb<<<grid_for(c.m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+        c.m, c.row_flp, c.ncol, ctx->d_counts + kSlotCursor, c.rows);
+    CAS_TRY(check_launch(ctx, "k_bin_scatter_symb"));
+  }
+  return CAS_OK;
+}
+
+// ------------------------------------------------------------------ SYMB
+cas_status launch_symb_bins(cas_ctx* ctx, Call& c, int64_t* row_nz) {
+  using namespace cas;
+  CAS_CUDA(ctx, cudaMemsetAsync(row_nz, 0, sizeof(int64_t) * (c.m + 1), ctx->stream));
+  CAS_TRY(fork(ctx));
+  int64_t off[kSymbBins + 1] = {0};
+  for (int b = 0; b < kSymbBins; ++b) off[b + 1] = off[b] + c.symb_count[b];
+  // heaviest bins first, each on its own stream
+  const int order[] = {kSB_Dense, kSB_H32K, kSB_H8K, kSB_H2K, kSB_H512, kSB_Tiny};
+  int si = 0;
+  for (int b : order) {
+    const int64_t n = c.symb_count[b];
+    if (n == 0) continue;
+    const int32_t* rows = c.rows + off[b];
+    cudaStream_t s = ctx->aux[si++ % kAux];
+    switch (b) {
+      case kSB_Tiny:
+        k_symb_tiny<256><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(rows, n, c.A.csr, c.B.csr, row_nz, ctx->d_status);
+        break;
+      case kSB_H512:
+        k_symb_hash<128, 9><<<(unsigned)n, 128, smem_symb_hash<128, 9>(), s>>>(rows, c.A.csr, c.B.csr, row_nz, ctx->d_status);
+        break;
+      case kSB_H2K:
+        k_symb_hash<256, 11><<<(unsigned)n, 256, smem_symb_hash<256, 11>(), s>>>(rows, c.A.csr, c.B.csr, row_nz, ctx->d_status);
+        break;
+      case kSB_H8K:
+        k_symb_hash<512, 13><<<(unsigned)n, 512, smem_symb_hash<512, 13>(), s>>>(rows, c.A.csr, c.B.csr, row_nz, ctx->d_status);
+        break;
+      case kSB_H32K:
+        k_symb_hash<1024, 15><<<(unsigned)n, 1024, smem_symb_hash<1024, 15>(), s>>>(rows, c.A.csr, c.B.csr, row_nz, ctx->d_status);
+        break;
+      case kSB_Dense:
+        if (!c.b_sorted && c.ncol > kDenseChunkBits)
+          return set_err(ctx, CAS_ERR_BAD_INPUT, "heavy rows over more than %d columns need B rows sorted by column", kDenseChunkBits);
+        k_symb_dense<1024><<<(unsigned)n, 1024, smem_symb_dense<1024>(), s>>>(rows, c.A.csr, c.B.csr, c.ncol, row_nz, ctx->d_status);
+        break;
+    }
+    CAS_TRY(check_launch(ctx, "symbolic bin"));
+  }
+  CAS_TRY(join(ctx));
+  return CAS_OK;
+}
+
+// ------------------------------------------------------------------ MGMT
+cas_status numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int mode) {
+  using namespace cas;
+  CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + kSlotNumc, 0, sizeof(unsigned long long) * kNumcBins, ctx->stream));
+  if (c.m > 0) {
+    k_bin_count_numc<<<grid_for(c.m, 256, ctx->sm_count * 8), 256, 0, ctx->stream>>>(
+        c.m, c.row_flp, crp, mode, ctx->acc_thres, ctx->d_counts + kSlotNumc);
+    CAS_TRY(check_launch(ctx, "k_bin_count_numc"));
+  }
+  CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotNumc, ctx->d_counts + kSlotNumc,
+                                sizeof(unsigned long long) * kNumcBins, cudaMemcpyDeviceToHost, ctx->stream));
+  CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  unsigned long long* cur = ctx->h_counts + kSlotCursor;
+  unsigned long long off = 0;
+  for (int b = 0; b < kNumcBins; ++b) {
+    c.numc_count[b] = (int64_t)ctx->h_counts[kSlotNumc + b];
+    cur[b] = off;
+    off += ctx->h_counts[kSlotNumc + b];
+  }
+  if (c.m > 0) {
+    CAS_CUDA(ctx, cudaMemcpyAsync(ctx->d_counts + kSlotCursor, cur, sizeof(unsigned long long) * kNumcBins,
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    k_bin_scatter_numc<<<grid_for(c.m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+        c.m, c.row_flp, crp, mode, ctx->acc_thres, ctx->d_counts + kSlotCursor, c.rows);
+    CAS_TRY(check_launch(ctx, "k_bin_scatter_numc"));
+  }
+  return CAS_OK;
+}
+
+// ------------------------------------------------------------------ NUMC
+template <typename VIn>
+cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* ccol, void* cval_v) {
+  using namespace cas;
+  using AT = typename Acc<VIn>::T;
+  AT* cval = static_cast<AT*>(cval_v);
+  CAS_TRY(fork(ctx));
+  int64_t off[kNumcBins + 1] = {0};
+  for (int b = 0; b < kNumcBins; ++b) off[b + 1] = off[b] + c.numc_count[b];
+  const int order[] = {kNB_Dense, kNB_E8K, kNB_H4K, kNB_E4K, kNB_H1K, kNB_E2K, kNB_E1K, kNB_H256, kNB_Tiny};
+  int si = 0;
+  for (int b : order) {
+    const int64_t n = c.numc_count[b];
+    if (n == 0) continue;
+    const int32_t* rows = c.rows + off[b];
+    cudaStream_t s = ctx->aux[si++ % kAux];
+    const Csr& A = c.A.csr;
+    const Csr& B = c.B.csr;
+    switch (b) {
+      case kNB_Tiny:
+        k_numc_tiny<256, VIn><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(rows, n, A, B, crp, ccol, cval, ctx->d_status);
+        break;
+      case kNB_E1K:
+        k_numc_esc<256, 1024, VIn><<<(unsigned)n, 256, smem_numc_esc<256, 1024, VIn>(), s>>>(rows, A, B, crp, ccol, cval, ctx->d_status);
+        break;
+      case kNB_E2K:
+        k_numc_esc<256, 2048, VIn><<<(unsigned)n, 256, smem_numc_esc<256, 2048, VIn>(), s>>>(rows, A, B, crp, ccol, cval, ctx->d_status);
+        break;
+      case kNB_E4K:
+        k_numc_esc<512, 4096, VIn><<<(unsigned)n, 512, smem_numc_esc<512, 4096, VIn>(), s>>>(rows, A, B, crp, ccol, cval, ctx->d_status);
+        break;
+      case kNB_E8K:
+        k_numc_esc<1024, 8192, VIn><<<(unsigned)n, 1024, smem_numc_esc<1024, 8192, VIn>(), s>>>(rows, A, B, crp, ccol, cval, ctx->d_status);
+        break;
+      case kNB_H256:
+        k_numc_hash<256, 9, VIn><<<(unsigned)n, 256, smem_numc_hash<256, 9, VIn>(), s>>>(rows, A, B, crp, ccol, cval, ctx->d_status);
+        break;
+      case kNB_H1K:
+        k_numc_hash<256, 11, VIn><<<(unsigned)n, 256, smem_numc_hash<256, 11, VIn>(), s>>>(rows, A, B, crp, ccol, cval, ctx->d_status);
+        break;
+      case kNB_H4K:
+        k_numc_hash<512, 13, VIn><<<(unsigned)n, 512, smem_numc_hash<512, 13, VIn>(), s>>>(rows, A, B, crp, ccol, cval, ctx->d_status);
+        break;
+      case kNB_Dense:
+        if (!c.b_sorted && c.ncol > kDenseChunkCols)
+          return set_err(ctx, CAS_ERR_BAD_INPUT, "heavy rows over more than %d columns need B rows sorted by column", kDenseChunkCols);
+        k_numc_dense<1024, VIn><<<(unsigned)n, 1024, smem_numc_dense<1024, VIn>(), s>>>(rows, A, B, c.ncol, crp, ccol, cval, ctx->d_status);
+        break;
+    }
+    CAS_TRY(check_launch(ctx, "numeric bin"));
+  }
+  CAS_TRY(join(ctx));
+  return CAS_OK;
+}
+
+int mode_of(cas_accum a) {
+  return a == CAS_ACC_HASH ? cas::kAccHash : (a == CAS_ACC_HSERSC ? cas::kAccEsc : cas::kAccHybrid);
+}
+
+cas_status prepare(cas_ctx* ctx, const cas_csr* A, const cas_csr* B, Call& c, double& h2d) {
+  CAS_TRY(basic_checks(ctx, A, "A"));
+  CAS_TRY(basic_checks(ctx, B, "B"));
+  if (A->num_col != B->num_row)
+    return set_err(ctx, CAS_ERR_BAD_INPUT, "A is %lldx%lld but B has %lld rows", (long long)A->num_row,
+                   (long long)A->num_col, (long long)B->num_row);
+  if (A->val_type != B->val_type) return set_err(ctx, CAS_ERR_BAD_INPUT, "A and B have different value types");
+  CAS_TRY(to_device(ctx, A, c.A, h2d));
+  CAS_TRY(to_device(ctx, B, c.B, h2d));
+  c.m = A->num_row;
+  c.ncol = B->num_col;
+  c.vt = A->val_type;
+  return CAS_OK;
+}
+
+cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas_csr* B, cas_csr* C,
+                      cas_runtime* rt) {
+  using namespace cas;
+  Call c;
+  double h2d = 0, d2h = 0;
+  const bool c_on_device = C->on_device != 0;
+  const int c_col_bytes = c_on_device ? 4 : (C->col_bytes == 8 ? 8 : 4);
+  CAS_TRY(prepare(ctx, A, B, c, h2d));
+  memset(C, 0, sizeof(*C));
+  const size_t vbytes = 8;  // fp64 or int64 output
+  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[0], ctx->stream));
+  // INIT
+  CAS_TRY(phase_init(ctx, c, true));
+  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[1], ctx->stream));
+  // SYMB
+  int64_t* crp = nullptr;
+  CAS_TRY(dev_alloc(ctx, (void**)&crp, sizeof(int64_t) * (c.m + 1)));
+  CAS_TRY(launch_symb_bins(ctx, c, c.row_nz));
+  CAS_TRY(launch_scan(ctx, crp, c.row_nz, c.m + 1, c.partial,
+                      reinterpret_cast<int64_t*>(ctx->d_counts + kSlotNnz)));
+  CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotNnz, ctx->d_counts + kSlotNnz, sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+  CAS_TRY(check_status(ctx));
+  const int64_t nnz = (int64_t)ctx->h_counts[kSlotNnz];
+  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[2], ctx->stream));
+  // MGMT
+  int32_t* ccol = nullptr;
+  void* cval = nullptr;
+  CAS_TRY(dev_alloc(ctx, (void**)&ccol, sizeof(int32_t) * nnz));
+  CAS_TRY(dev_alloc(ctx, &cval, vbytes * nnz));
+  CAS_TRY(numc_bins(ctx, c, crp, mode_of(accum)));
+  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[3], ctx->stream));
+  // NUMC
+  if (c.vt == CAS_VAL_F64) CAS_TRY(launch_numc_bins<double>(ctx, c, crp, ccol, cval));
+  else CAS_TRY(launch_numc_bins<int32_t>(ctx, c, crp, ccol, cval));
+  CAS_TRY(scratch_free(ctx, c));
+  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[4], ctx->stream));
+  CAS_TRY(check_status(ctx));
+  CAS_TRY(free_owned(ctx, c.A));
+  CAS_TRY(free_owned(ctx, c.B));
+
+  C->num_row = c.m;
+  C->num_col = c.ncol;
+  C->num_nnz = nnz;
+  C->val_type = c.vt;
+  C->owned = 1;
+  if (c_on_device) {
+    C->on_device = 1;
+    C->col_bytes = 4;
+    C->row_ptrs = crp;
+    C->cols = ccol;
+    C->rats = cval;
+  } else {
+    C->on_device = 0;
+    C->col_bytes = c_col_bytes;
+    C->row_ptrs = static_cast<int64_t*>(malloc(sizeof(int64_t) * (c.m + 1)));
+    C->cols = malloc((size_t)c_col_bytes * (nnz > 0 ? nnz : 1));
+    C->rats = malloc(vbytes * (nnz > 0 ? nnz : 1));
+    if (!C->row_ptrs || !C->cols || !C->rats) {
+      free(C->row_ptrs); free(C->cols); free(C->rats);
+      memset(C, 0, sizeof(*C));
+      return set_err(ctx, CAS_ERR_OOM, "host allocation of C failed");
+    }
+    CAS_CUDA(ctx, cudaMemcpyAsync(C->row_ptrs, crp, sizeof(int64_t) * (c.m + 1), cudaMemcpyDeviceToHost, ctx->stream));
+    CAS_CUDA(ctx, cudaMemcpyAsync(C->rats, cval, vbytes * nnz, cudaMemcpyDeviceToHost, ctx->stream));
+    if (c_col_bytes == 4) {
+      CAS_CUDA(ctx, cudaMemcpyAsync(C->cols, ccol, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, ctx->stream));
+      CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    } else {
+      std::vector<int32_t> tmp((size_t)nnz);
+      CAS_CUDA(ctx, cudaMemcpyAsync(tmp.data(), ccol, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, ctx->stream));
+      CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      int64_t* c64 = static_cast<int64_t*>(C->cols);
+      for (int64_t i = 0; i < nnz; ++i) c64[i] = tmp[(size_t)i];
+    }
+    d2h += sizeof(int64_t) * (double)(c.m + 1) + (vbytes + c_col_bytes) * (double)nnz;
+    CAS_CUDA(ctx, cudaFreeAsync(crp, ctx->stream));
+    CAS_CUDA(ctx, cudaFreeAsync(ccol, ctx->stream));
+    CAS_CUDA(ctx, cudaFreeAsync(cval, ctx->stream));
+    CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  float ms[4];
+  for (int i = 0; i < 4; ++i) CAS_CUDA(ctx, cudaEventElapsedTime(&ms[i], ctx->ev_phase[i], ctx->ev_phase[i + 1]));
+  if (rt) {
+    rt->init_time = ms[0] * 1e-3;
+    rt->symb_time = ms[1] * 1e-3;
+    rt->mgmt_time = ms[2] * 1e-3;
+    rt->numc_time = ms[3] * 1e-3;
+    rt->total_time = rt->init_time + rt->symb_time + rt->mgmt_time + rt->numc_time;
+  }
+  cas_stats& s = ctx->stats;
+  s.flop = c.flop;
+  s.max_row_flp = c.max_flp;
+  s.nnz_c = nnz;
+  for (int b = 0; b < kSymbBins; ++b) s.symb_bin_rows[b] = c.symb_count[b];
+  for (int b = 0; b < kNumcBins; ++b) s.numc_bin_rows[b] = c.numc_count[b];
+  s.kernel_launches = ctx->launches;
+  s.h2d_bytes = h2d;
+  s.d2h_bytes = d2h;
+  return CAS_OK;
+}
+
+}  // namespace
+
+// ================================================================= C ABI
+extern "C" {
+
+cas_status cas_create(int device, cas_ctx** out) {
+  if (!out) return CAS_ERR_BAD_INPUT;
+  *out = nullptr;
+  cas_ctx* ctx = new (std::nothrow) cas_ctx();
+  if (!ctx) return CAS_ERR_OOM;
+  ctx->device = device;
+  cas_status st = [&]() -> cas_status {
+    CAS_CUDA(ctx, cudaSetDevice(device));
+    CAS_CUDA(ctx, cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
+    CAS_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
+    ctx->stream = ctx->own_stream;
+    for (int i = 0; i < kAux; ++i) {
+      CAS_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->aux[i], cudaStreamNonBlocking));
+      CAS_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming));
+    }
+    CAS_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+    for (int i = 0; i < 5; ++i) CAS_CUDA(ctx, cudaEventCreate(&ctx->ev_phase[i]));
+    CAS_CUDA(ctx, cudaMalloc(&ctx->d_status, sizeof(cas::DevStatus)));
+    CAS_CUDA(ctx, cudaMalloc(&ctx->d_counts, sizeof(unsigned long long) * kCountSlots));
+    CAS_CUDA(ctx, cudaMallocHost(&ctx->h_counts, sizeof(unsigned long long) * kCountSlots));
+    CAS_CUDA(ctx, cudaMallocHost(&ctx->h_status, sizeof(cas::DevStatus)));
+    // keep freed device memory in the stream-ordered pool between calls
+    cudaMemPool_t pool;
+    CAS_CUDA(ctx, cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t thresh = UINT64_MAX;
+    CAS_CUDA(ctx, cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thresh));
+    CAS_TRY(setup_kernels(ctx));
+    return CAS_OK;
+  }();
+  if (st != CAS_OK) {
+    fprintf(stderr, "cas_create: %s\n", ctx->err.c_str());
+    cas_destroy(ctx);
+    return st;
+  }
+  *out = ctx;
+  return CAS_OK;
+}
+
+void cas_destroy(cas_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
+  for (int i = 0; i < kAux; ++i) {
+    if (ctx->aux[i]) cudaStreamDestroy(ctx->aux[i]);
+    if (ctx->ev_join[i]) cudaEventDestroy(ctx->ev_join[i]);
+  }
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  for (int i = 0; i < 5; ++i)
+    if (ctx->ev_phase[i]) cudaEventDestroy(ctx->ev_phase[i]);
+  if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->d_counts) cudaFree(ctx->d_counts);
+  if (ctx->h_counts) cudaFreeHost(ctx->h_counts);
+  if (ctx->h_status) cudaFreeHost(ctx->h_status);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+}
+
+cas_status cas_set_stream(cas_ctx* ctx, void* stream) {
+  if (!ctx) return CAS_ERR_BAD_INPUT;
+  ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+  return CAS_OK;
+}
+
+cas_status cas_set_acc_thres(cas_ctx* ctx, double thres) {
+  if (!ctx || !(thres >= 0.0)) return CAS_ERR_BAD_INPUT;
+  ctx->acc_thres = thres;
+  return CAS_OK;
+}
+
+const char* cas_last_error(const cas_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+cas_status cas_get_stats(const cas_ctx* ctx, cas_stats* out) {
+  if (!ctx || !out) return CAS_ERR_BAD_INPUT;
+  *out = ctx->stats;
+  out->kernel_launches = ctx->launches;
+  return CAS_OK;
+}
+
+cas_status cas_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas_csr* B, cas_csr* C,
+                      cas_runtime* rt) {
+  if (!ctx || !C) return CAS_ERR_BAD_INPUT;
+  if (accum != CAS_ACC_HASH && accum != CAS_ACC_HSERSC && accum != CAS_ACC_HYBACC)
+    return set_err(ctx, CAS_ERR_BAD_INPUT, "unknown accumulator %d", (int)accum);
+  CAS_CUDA(ctx, cudaSetDevice(ctx->device));
+  return run_spgemm(ctx, accum, A, B, C, rt);
+}
+
+cas_status cas_csr_free(cas_ctx* ctx, cas_csr* C) {
+  if (!C) return CAS_ERR_BAD_INPUT;
+  if (C->owned) {
+    if (C->on_device) {
+      if (ctx) {
+        cudaStream_t s = ctx->stream;
+        cudaFreeAsync(C->row_ptrs, s);
+        cudaFreeAsync(C->cols, s);
+        cudaFreeAsync(C->rats, s);
+        cudaStreamSynchronize(s);
+      } else {
+        cudaFree(C->row_ptrs);
+        cudaFree(C->cols);
+        cudaFree(C->rats);
+      }
+    } else {
+      free(C->row_ptrs);
+      free(C->cols);
+      free(C->rats);
+    }
+  }
+  memset(C, 0, sizeof(*C));
+  return CAS_OK;
+}
+
+// ---- phase functions ---------------------------------------------------
+
+cas_status cas_flp_populate(cas_ctx* ctx, const cas_csr* A, const cas_csr* B, int64_t* d_row_flp) {
+  if (!ctx || !d_row_flp) return CAS_ERR_BAD_INPUT;
+  if (!A || !B || !A->on_device || !B->on_device)
+    return set_err(ctx, CAS_ERR_BAD_INPUT, "phase functions take device matrices");
+  Call c;
+  double h2d = 0;
+  CAS_TRY(prepare(ctx, A, B, c, h2d));
+  CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_counts, 0, sizeof(unsigned long long) * kCountSlots, ctx->stream));
+  CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(cas::DevStatus), ctx->stream));
+  if (c.m > 0) {
+    cas::k_flp<256><<<grid_for(c.m * 32, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+        c.A.csr, c.B.csr, c.ncol, d_row_flp, ctx->d_counts + kSlotTotals, ctx->d_counts + kSlotSymb, ctx->d_status);
+    CAS_TRY(check_launch(ctx, "k_flp"));
+  }
+  return check_status(ctx);
+}
+
+cas_status cas_scan(cas_ctx* ctx, int64_t* d_out, const int64_t* d_in, int64_t n) {
+  if (!ctx || !d_out || (n > 1 && !d_in) || n < 0) return CAS_ERR_BAD_INPUT;
+  if (n == 0) return CAS_OK;
+  const int64_t nparts = (n + cas::kScanTile - 1) / cas::kScanTile;
+  int64_t* partial = nullptr;
+  CAS_TRY(dev_alloc(ctx, (void**)&partial, sizeof(int64_t) * (nparts + 1)));
+  cas_status st = launch_scan(ctx, d_out, d_in, n, partial, nullptr);
+  CAS_CUDA(ctx, cudaFreeAsync(partial, ctx->stream));
+  CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return st;
+}
+
+cas_status cas_hash_symb(cas_ctx* ctx, const cas_csr* A, const cas_csr* B, const int64_t* d_row_flp,
+                         int64_t* d_row_nz) {
+  if (!ctx || !d_row_nz) return CAS_ERR_BAD_INPUT;
+  if (!A || !B || !A->on_device || !B->on_device)
+    return set_err(ctx, CAS_ERR_BAD_INPUT, "phase functions take device matrices");
+  (void)d_row_flp;  // recomputed together with the bins
+  Call c;
+  double h2d = 0;
+  CAS_TRY(prepare(ctx, A, B, c, h2d));
+  CAS_TRY(phase_init(ctx, c, true));
+  CAS_TRY(launch_symb_bins(ctx, c, d_row_nz));
+  CAS_TRY(scratch_free(ctx, c));
+  return check_status(ctx);
+}
+
+static cas_status numc_entry(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas_csr* B, cas_csr* C) {
+  if (!ctx || !C) return CAS_ERR_BAD_INPUT;
+  if (!A || !B || !A->on_device || !B->on_device || !C->on_device)
+    return set_err(ctx, CAS_ERR_BAD_INPUT, "phase functions take device matrices");
+  Call c;
+  double h2d = 0;
+  CAS_TRY(prepare(ctx, A, B, c, h2d));
+  CAS_TRY(phase_init(ctx, c, true));
+  CAS_TRY(numc_bins(ctx, c, C->row_ptrs, mode_of(accum)));
+  if (c.vt == CAS_VAL_F64)
+    CAS_TRY(launch_numc_bins<double>(ctx, c, C->row_ptrs, static_cast<int32_t*>(C->cols), C->rats));
+  else
+    CAS_TRY(launch_numc_bins<int32_t>(ctx, c, C->row_ptrs, static_cast<int32_t*>(C->cols), C->rats));
+  CAS_TRY(scratch_free(ctx, c));
+  return check_status(ctx);
+}
+
+cas_status cas_hash_numc(cas_ctx* ctx, const cas_csr* A, const cas_csr* B, const int64_t* d_row_flp, cas_csr* C) {
+  (void)d_row_flp;
+  return numc_entry(ctx, CAS_ACC_HASH, A, B, C);
+}
+cas_status cas_hsersc_numc(cas_ctx* ctx, const cas_csr* A, const cas_csr* B, const int64_t* d_row_flp, cas_csr* C) {
+  (void)d_row_flp;
+  return numc_entry(ctx, CAS_ACC_HSERSC, A, B, C);
+}
+cas_status cas_hybacc_numc(cas_ctx* ctx, const cas_csr* A, const cas_csr* B, const int64_t* d_row_flp, cas_csr* C) {
+  (void)d_row_flp;
+  return numc_entry(ctx, CAS_ACC_HYBACC, A, B, C);
+}
+
+}  // extern "C"

@@ -1,0 +1,654 @@
+// casgemm kernel bodies (contracts in cas_kernels.cuh).
+#include "cas_kernels.cuh"
+
+namespace cas {
+
+// ===================================================================== INIT
+
+// One warp per row of A: row_flp[i] = sum over A_i of |B_k|, the symbolic
+// bin histogram, and the block-reduced total and maximum.  Columns outside
+// [0, B.nrow) are reported and skipped.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_flp(Csr A, Csr B, int64_t c_ncol, int64_t* __restrict__ row_flp,
+      unsigned long long* __restrict__ totals, unsigned long long* __restrict__ bin_count,
+      DevStatus* st) {
+  __shared__ unsigned long long s_cnt[kSymbBins];
+  __shared__ unsigned long long s_tot, s_max;
+  if (threadIdx.x < kSymbBins) s_cnt[threadIdx.x] = 0;
+  if (threadIdx.x == 0) { s_tot = 0; s_max = 0; }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * BLOCK) >> 5;
+  unsigned long long my_tot = 0, my_max = 0;
+  for (int64_t r = ((int64_t)blockIdx.x * BLOCK + threadIdx.x) >> 5; r < A.nrow; r += nw) {
+    const int64_t s = A.rp[r], e = A.rp[r + 1];
+    long long sum = 0;
+    for (int64_t j = s + lane; j < e; j += 32) {
+      const int32_t k = A.col[j];
+      if ((uint64_t)k >= (uint64_t)B.nrow) {
+        dev_report(st, kDevBadIndex, 0, r);
+        continue;
+      }
+      sum += B.rp[k + 1] - B.rp[k];
+    }
+    sum = warp_sum(sum);
+    if (lane == 0) {
+      row_flp[r] = sum;
+      my_tot += (unsigned long long)sum;
+      my_max = max(my_max, (unsigned long long)sum);
+      atomicAdd(&s_cnt[symb_bin_of(sum, c_ncol)], 1ull);
+    }
+  }
+  if (lane == 0) {
+    atomicAdd(&s_tot, my_tot);
+    atomicMax(&s_max, my_max);
+  }
+  __syncthreads();
+  if (threadIdx.x < kSymbBins && s_cnt[threadIdx.x]) atomicAdd(&bin_count[threadIdx.x], s_cnt[threadIdx.x]);
+  if (threadIdx.x == 0) {
+    atomicAdd(&totals[0], s_tot);
+    atomicMax(&totals[1], s_max);
+  }
+}
+
+// Rows into per-bin lists.  cursor[b] starts at the bin's offset; lanes that
+// hit the same bin share one atomic (warp-aggregated).
+__global__ void k_bin_scatter_symb(int64_t m, const int64_t* __restrict__ row_flp, int64_t c_ncol,
+                                   unsigned long long* __restrict__ cursor, int32_t* __restrict__ rows) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
+    const int b = symb_bin_of(row_flp[r], c_ncol);
+    const unsigned long long pos = warp_aggregated_add(cursor, b);
+    rows[pos] = (int32_t)r;
+  }
+}
+
+__global__ void k_bin_count_numc(int64_t m, const int64_t* __restrict__ row_flp, const int64_t* __restrict__ crp,
+                                 int mode, double thres, unsigned long long* __restrict__ bin_count) {
+  __shared__ unsigned long long s_cnt[kNumcBins];
+  if (threadIdx.x < kNumcBins) s_cnt[threadIdx.x] = 0;
+  __syncthreads();
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
+    const int b = numc_bin_of(row_flp[r], crp[r + 1] - crp[r], mode, thres);
+    atomicAdd(&s_cnt[b], 1ull);
+  }
+  __syncthreads();
+  if (threadIdx.x < kNumcBins && s_cnt[threadIdx.x]) atomicAdd(&bin_count[threadIdx.x], s_cnt[threadIdx.x]);
+}
+
+__global__ void k_bin_scatter_numc(int64_t m, const int64_t* __restrict__ row_flp, const int64_t* __restrict__ crp,
+                                   int mode, double thres, unsigned long long* __restrict__ cursor,
+                                   int32_t* __restrict__ rows) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
+    const int b = numc_bin_of(row_flp[r], crp[r + 1] - crp[r], mode, thres);
+    const unsigned long long pos = warp_aggregated_add(cursor, b);
+    rows[pos] = (int32_t)r;
+  }
+}
+
+// ===================================================================== scan
+// Exclusive scan out[0..n) of in[0..n-1): out[0] = 0, out[i+1] = out[i] + in[i]
+// (the contract of scan, src/mm/mm_utils.c:903-911).  Reduce-then-scan over
+// tiles of BLOCK*ITEMS: no inter-block waiting.
+constexpr int kScanBlock = 512;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanBlock * kScanItems;
+
+__global__ void __launch_bounds__(kScanBlock)
+k_scan_partials(const int64_t* __restrict__ in, int64_t n_in, int64_t* __restrict__ partial) {
+  __shared__ long long tmp[kScanBlock / 32 + 1];
+  const int64_t base = (int64_t)blockIdx.x * kScanTile;
+  long long s = 0;
+#pragma unroll
+  for (int u = 0; u < kScanItems; ++u) {
+    const int64_t i = base + (int64_t)u * kScanBlock + threadIdx.x;
+    if (i < n_in) s += in[i];
+  }
+  s = block_sum<kScanBlock, long long>(s, tmp);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+// single block: exclusive scan of the tile partials (any count, in rounds)
+__global__ void __launch_bounds__(kScanBlock)
+k_scan_top(int64_t* __restrict__ partial, int64_t nparts, int64_t* __restrict__ total_out) {
+  __shared__ long long tmp[kScanBlock / 32 + 1];
+  long long carry = 0;
+  for (int64_t b0 = 0; b0 < nparts; b0 += kScanBlock) {
+    const int64_t i = b0 + threadIdx.x;
+    const long long v = i < nparts ? partial[i] : 0;
+    long long tot;
+    const long long ex = block_exclusive_sum<kScanBlock, long long>(v, tmp, tot);
+    if (i < nparts) partial[i] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0 && total_out) *total_out = carry;
+}
+
+__global__ void __launch_bounds__(kScanBlock)
+k_scan_apply(const int64_t* __restrict__ in, int64_t n_in, const int64_t* __restrict__ partial,
+             int64_t* __restrict__ out, int64_t n_out) {
+  __shared__ long long tmp[kScanBlock / 32 + 1];
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  long long v[kScanItems];
+  long long s = 0;
+#pragma unroll
+  for (int u = 0; u < kScanItems; ++u) {
+    const int64_t i = base + u;
+    v[u] = i < n_in ? in[i] : 0;
+    s += v[u];
+  }
+  long long tot;
+  long long run = block_exclusive_sum<kScanBlock, long long>(s, tmp, tot) + partial[blockIdx.x];
+#pragma unroll
+  for (int u = 0; u < kScanItems; ++u) {
+    const int64_t i = base + u;
+    if (i < n_out) out[i] = run;
+    run += v[u];
+  }
+}
+
+// ============================================================ row expansion
+// Enumerates the products of one row of A*B inside a thread block: A entries
+// are staged min(BLOCK, kAChunk) at a time (B row start, length, A value), their lengths
+// scanned, and each thread then takes products p = tid, tid+BLOCK, ... and
+// finds its A entry by binary search, so work is balanced whatever the B row
+// lengths.  Loads of U products are issued before any is consumed.  With
+// `ranged`, every B row is cut to the columns [c0, c1) by binary search (B
+// rows sorted); otherwise f receives every product.
+constexpr int kAChunk = 256;
+constexpr int kUnroll = 4;
+
+template <typename VIn>
+struct alignas(16) Stage {
+  int64_t bs[kAChunk];
+  int64_t pre[kAChunk + 1];
+  VIn av[kAChunk];
+  long long tmp[33];
+};
+
+template <int BLOCK, bool NEED_VAL, typename VIn, typename F>
+__device__ __forceinline__ int64_t expand_row(const Csr& A, const Csr& B, int64_t r, Stage<VIn>& sg,
+                                              bool ranged, int32_t c0, int32_t c1, F&& f) {
+  const int64_t as = A.rp[r], ae = A.rp[r + 1];
+  const VIn* __restrict__ aval = static_cast<const VIn*>(A.val);
+  const VIn* __restrict__ bval = static_cast<const VIn*>(B.val);
+  constexpr int ACH = BLOCK < kAChunk ? BLOCK : kAChunk;  // one staged A entry per thread
+  int64_t pbase = 0;
+  for (int64_t a0 = as; a0 < ae; a0 += ACH) {
+    const int na = (int)((ae - a0) < (int64_t)ACH ? (ae - a0) : (int64_t)ACH);
+    long long len = 0;
+    if (threadIdx.x < na) {
+      const int32_t k = A.col[a0 + threadIdx.x];
+      int64_t lo = B.rp[k], hi = B.rp[k + 1];
+      if (ranged) {
+        lo = lower_bound_g(B.col, lo, hi, c0);
+        hi = lower_bound_g(B.col, lo, hi, c1);
+      }
+      sg.bs[threadIdx.x] = lo;
+      len = hi - lo;
+      if (NEED_VAL) sg.av[threadIdx.x] = aval[a0 + threadIdx.x];
+    }
+    long long total;
+    const long long ex = block_exclusive_sum<BLOCK, long long>(len, sg.tmp, total);
+    if (threadIdx.x < ACH) sg.pre[threadIdx.x] = ex;
+    __syncthreads();
+    for (int64_t p0 = threadIdx.x; p0 < total; p0 += (int64_t)BLOCK * kUnroll) {
+      int32_t key[kUnroll];
+      VIn bv[kUnroll];
+      int sgi[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const int64_t p = p0 + (int64_t)u * BLOCK;
+        sgi[u] = -1;
+        if (p < total) {
+          int lo = 0, hi = na;
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (sg.pre[mid] <= p) lo = mid; else hi = mid;
+          }
+          const int64_t j = sg.bs[lo] + (p - sg.pre[lo]);
+          key[u] = __ldg(B.col + j);
+          if (NEED_VAL) bv[u] = __ldg(bval + j);
+          sgi[u] = lo;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        if (sgi[u] >= 0) {
+          if (!ranged || (key[u] >= c0 && key[u] < c1)) {
+            if (NEED_VAL) f(key[u], sg.av[sgi[u]], bv[u], pbase + p0 + (int64_t)u * BLOCK);
+            else f(key[u], VIn(0), VIn(0), pbase + p0 + (int64_t)u * BLOCK);
+          }
+        }
+      }
+    }
+    pbase += total;
+    __syncthreads();
+  }
+  return pbase;
+}
+
+// ================================================================ SYMBOLIC
+
+// Rows with at most 32 products: one warp per row, one product per lane; the
+// distinct count is the number of lanes that lead their __match_any_sync group.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_symb_tiny(const int32_t* __restrict__ rows, int64_t nrows, Csr A, Csr B, int64_t* __restrict__ row_nz,
+            DevStatus* st) {
+  __shared__ int64_t s_bs[BLOCK];
+  __shared__ int32_t s_ex[BLOCK];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int64_t* wbs = s_bs + wib * 32;
+  int32_t* wex = s_ex + wib * 32;
+  const int64_t w = ((int64_t)blockIdx.x * BLOCK + threadIdx.x) >> 5;
+  if (w >= nrows) return;
+  const int64_t r = rows[w];
+  const int64_t as = A.rp[r], ae = A.rp[r + 1];
+  uint64_t mykey = (1ull << 32) | (uint64_t)lane;  // unique dummy for empty lanes
+  int base = 0;
+  for (int64_t a0 = as; a0 < ae; a0 += 32) {
+    const int64_t ja = a0 + lane;
+    int32_t len = 0;
+    int64_t bs = 0;
+    if (ja < ae) {
+      const int32_t k = A.col[ja];
+      bs = B.rp[k];
+      len = (int32_t)(B.rp[k + 1] - bs);
+    }
+    const int32_t inc = warp_inclusive_sum(len);
+    const int32_t tot = __shfl_sync(kFull, inc, 31);
+    wbs[lane] = bs;
+    wex[lane] = inc - len;
+    __syncwarp();
+    const int p = lane - base;
+    if (p >= 0 && p < tot) {
+      int lo = 0, hi = 32;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (wex[mid] <= p) lo = mid; else hi = mid;
+      }
+      mykey = (uint64_t)(uint32_t)__ldg(B.col + wbs[lo] + (p - wex[lo]));
+    }
+    base += tot;
+    __syncwarp();
+  }
+  if (base > 32 && lane == 0) dev_report(st, kDevCapacity, 1, r);
+  const unsigned peers = __match_any_sync(kFull, mykey);
+  const bool lead = (mykey >> 32) == 0 && lane == __ffs(peers) - 1;
+  const int cnt = __popc(__ballot_sync(kFull, lead));
+  if (lane == 0) row_nz[r] = cnt;
+}
+
+// Rows whose distinct columns fit a shared-memory hash of 2^TBITS keys (at
+// least twice the bound min(row_flp, num_col)): linear probing on 32-bit keys,
+// one atomicCAS per new key; the count is the number of successful inserts
+// (ams_hash_symb_krnl, src/ams/ams_utils.c:101-164, in shared memory).
+template <int BLOCK, int TBITS>
+__global__ void __launch_bounds__(BLOCK)
+k_symb_hash(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t* __restrict__ row_nz, DevStatus* st) {
+  constexpr int T = 1 << TBITS;
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint32_t* tab = reinterpret_cast<uint32_t*>(smem);
+  Stage<double>& sg = *reinterpret_cast<Stage<double>*>(smem + T * sizeof(uint32_t));
+  const int64_t r = rows[blockIdx.x];
+  for (int i = threadIdx.x; i < T; i += BLOCK) tab[i] = kEmptyKey;
+  __syncthreads();
+  long long cnt = 0;
+  bool full = false;
+  expand_row<BLOCK, false, double>(A, B, r, sg, false, 0, 0, [&](int32_t key, double, double, int64_t) {
+    uint32_t h = hash_slot((uint32_t)key, TBITS);
+    for (int probe = 0; probe < T; ++probe) {
+      const uint32_t cur = tab[h];
+      if (cur == (uint32_t)key) return;
+      if (cur == kEmptyKey) {
+        const uint32_t old = atomicCAS(&tab[h], kEmptyKey, (uint32_t)key);
+        if (old == kEmptyKey) { ++cnt; return; }
+        if (old == (uint32_t)key) return;
+      }
+      h = (h + 1) & (T - 1);
+    }
+    full = true;
+  });
+  if (full) dev_report(st, kDevTableFull, 2, r);
+  cnt = block_sum<BLOCK, long long>(cnt, sg.tmp);
+  if (threadIdx.x == 0) row_nz[r] = cnt;
+}
+
+// Heavy rows: a bitmap over kDenseChunkBits columns at a time; the count is
+// the population count.  B rows are cut to each column chunk by binary search
+// when there is more than one chunk.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_symb_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int64_t* __restrict__ row_nz,
+             DevStatus* st) {
+  constexpr int W = kDenseChunkBits / 32;
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint32_t* bm = reinterpret_cast<uint32_t*>(smem);
+  Stage<double>& sg = *reinterpret_cast<Stage<double>*>(smem + W * sizeof(uint32_t));
+  const int64_t r = rows[blockIdx.x];
+  const bool multi = c_ncol > kDenseChunkBits;
+  long long cnt = 0;
+  for (int64_t c0 = 0; c0 < c_ncol; c0 += kDenseChunkBits) {
+    const int64_t c1 = (c_ncol < c0 + kDenseChunkBits ? c_ncol : c0 + kDenseChunkBits);
+    for (int i = threadIdx.x; i < W; i += BLOCK) bm[i] = 0u;
+    __syncthreads();
+    bool bad = false;
+    expand_row<BLOCK, false, double>(A, B, r, sg, multi, (int32_t)c0, (int32_t)c1,
+                                     [&](int32_t key, double, double, int64_t) {
+      const int64_t idx = (int64_t)key - c0;
+      if (idx < 0 || idx >= kDenseChunkBits) { bad = true; return; }
+      atomicOr(&bm[idx >> 5], 1u << (idx & 31));
+    });
+    if (bad && !multi) dev_report(st, kDevBadIndex, 3, r);
+    __syncthreads();
+    for (int i = threadIdx.x; i < W; i += BLOCK) cnt += __popc(bm[i]);
+    __syncthreads();
+  }
+  cnt = block_sum<BLOCK, long long>(cnt, sg.tmp);
+  if (threadIdx.x == 0) row_nz[r] = cnt;
+}
+
+// ================================================================= NUMERIC
+
+// Rows with at most 32 products: one product per lane, a 32-lane bitonic sort
+// by column in registers, a segmented sum from the right, and one store per
+// distinct column (the ESC accumulator at warp scale).
+template <int BLOCK, typename VIn>
+__global__ void __launch_bounds__(BLOCK)
+k_numc_tiny(const int32_t* __restrict__ rows, int64_t nrows, Csr A, Csr B, const int64_t* __restrict__ crp,
+            int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval, DevStatus* st) {
+  using AT = typename Acc<VIn>::T;
+  __shared__ int64_t s_bs[BLOCK];
+  __shared__ int32_t s_ex[BLOCK];
+  __shared__ VIn s_av[BLOCK];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int64_t* wbs = s_bs + wib * 32;
+  int32_t* wex = s_ex + wib * 32;
+  VIn* wav = s_av + wib * 32;
+  const int64_t w = ((int64_t)blockIdx.x * BLOCK + threadIdx.x) >> 5;
+  if (w >= nrows) return;
+  const int64_t r = rows[w];
+  const int64_t as = A.rp[r], ae = A.rp[r + 1];
+  const VIn* __restrict__ aval = static_cast<const VIn*>(A.val);
+  const VIn* __restrict__ bval = static_cast<const VIn*>(B.val);
+  uint32_t key = kEmptyKey;
+  AT val = AT(0);
+  int base = 0;
+  for (int64_t a0 = as; a0 < ae; a0 += 32) {
+    const int64_t ja = a0 + lane;
+    int32_t len = 0;
+    int64_t bs = 0;
+    VIn av = VIn(0);
+    if (ja < ae) {
+      const int32_t k = A.col[ja];
+      bs = B.rp[k];
+      len = (int32_t)(B.rp[k + 1] - bs);
+      av = aval[ja];
+    }
+    const int32_t inc = warp_inclusive_sum(len);
+    const int32_t tot = __shfl_sync(kFull, inc, 31);
+    wbs[lane] = bs;
+    wex[lane] = inc - len;
+    wav[lane] = av;
+    __syncwarp();
+    const int p = lane - base;
+    if (p >= 0 && p < tot) {
+      int lo = 0, hi = 32;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (wex[mid] <= p) lo = mid; else hi = mid;
+      }
+      const int64_t j = wbs[lo] + (p - wex[lo]);
+      key = (uint32_t)__ldg(B.col + j);
+      val = Acc<VIn>::mul(wav[lo], __ldg(bval + j));
+    }
+    base += tot;
+    __syncwarp();
+  }
+  // bitonic sort of (key, val) across the warp, ascending by key
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const uint32_t ok = __shfl_xor_sync(kFull, key, j);
+      const AT ov = __shfl_xor_sync(kFull, val, j);
+      const bool up = (lane & k) == 0;
+      const bool lower = (lane & j) == 0;
+      const bool take = lower ? (up ? ok < key : ok > key) : (up ? ok > key : ok < key);
+      if (take) { key = ok; val = ov; }
+    }
+  }
+  // segmented sum toward each run's first lane
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t ok = __shfl_down_sync(kFull, key, d);
+    const AT ov = __shfl_down_sync(kFull, val, d);
+    if (lane + d < 32 && ok == key) val += ov;
+  }
+  const uint32_t prev = __shfl_up_sync(kFull, key, 1);
+  const bool head = key != kEmptyKey && (lane == 0 || prev != key);
+  const unsigned heads = __ballot_sync(kFull, head);
+  const int64_t c0 = crp[r], nz = crp[r + 1] - c0;
+  const int pos = __popc(heads & lanemask_lt());
+  if (head && pos < nz) {
+    ccol[c0 + pos] = (int32_t)key;
+    cval[c0 + pos] = val;
+  }
+  if (lane == 0 && __popc(heads) != nz) dev_report(st, __popc(heads) > nz ? kDevRowOverflow : kDevRowUnderflow, 10, r);
+}
+
+// Shared-memory layout helpers for the sort-based kernels.
+template <int BLOCK>
+struct alignas(16) SortScratch {
+  uint16_t hist[(BLOCK / 32) * 256];
+  int tmp[33];
+};
+
+// ESC accumulator for rows of at most CAP products: expand (column, a*b) into
+// shared memory, sort by column with the block radix sort, and sum runs of
+// equal columns (ams_hsersc_numc_krnl, src/ams/ams_utils.c:399-456).  The
+// sort is stable, so each sum is taken in expansion order.
+template <int BLOCK, int CAP, typename VIn>
+__global__ void __launch_bounds__(BLOCK)
+k_numc_esc(const int32_t* __restrict__ rows, Csr A, Csr B, const int64_t* __restrict__ crp,
+           int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval, DevStatus* st) {
+  using AT = typename Acc<VIn>::T;
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint64_t* items = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* items2 = items + CAP;
+  AT* ev = reinterpret_cast<AT*>(items2 + CAP);
+  SortScratch<BLOCK>& ss = *reinterpret_cast<SortScratch<BLOCK>*>(ev + CAP);
+  Stage<VIn>& sg = *reinterpret_cast<Stage<VIn>*>(reinterpret_cast<uint8_t*>(&ss) + sizeof(SortScratch<BLOCK>));
+  __shared__ uint32_t s_min, s_max;
+  __shared__ int s_over;
+  const int64_t r = rows[blockIdx.x];
+  if (threadIdx.x == 0) { s_min = 0xFFFFFFFFu; s_max = 0u; s_over = 0; }
+  __syncthreads();
+  uint32_t kmin = 0xFFFFFFFFu, kmax = 0u;
+  bool over = false;
+  const int64_t n = expand_row<BLOCK, true, VIn>(A, B, r, sg, false, 0, 0,
+                                                [&](int32_t key, VIn av, VIn bv, int64_t p) {
+    if (p >= CAP) { over = true; return; }
+    items[p] = ((uint64_t)(uint32_t)key << 32) | (uint64_t)p;
+    ev[p] = Acc<VIn>::mul(av, bv);
+    kmin = min(kmin, (uint32_t)key);
+    kmax = max(kmax, (uint32_t)key);
+  });
+  kmin = warp_min_u32(kmin);
+  kmax = warp_max_u32(kmax);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&s_min, kmin);
+    atomicMax(&s_max, kmax);
+    if (over) s_over = 1;
+  }
+  __syncthreads();
+  const int64_t c0 = crp[r], nz = crp[r + 1] - c0;
+  if (s_over || n > CAP) {
+    if (threadIdx.x == 0) dev_report(st, kDevCapacity, 11, r);
+    return;
+  }
+  const int nn = (int)n;
+  const uint64_t* sorted = block_radix_sort<BLOCK>(items, items2, nn, s_min, s_max, ss.hist, ss.tmp);
+  int carry = 0;
+  for (int t0 = 0; t0 < nn; t0 += BLOCK) {
+    const int t = t0 + threadIdx.x;
+    uint32_t key = 0;
+    bool head = false;
+    if (t < nn) {
+      key = (uint32_t)(sorted[t] >> 32);
+      head = t == 0 || (uint32_t)(sorted[t - 1] >> 32) != key;
+    }
+    int tot;
+    const int ex = block_exclusive_sum<BLOCK, int>(head ? 1 : 0, ss.tmp, tot);
+    if (head) {
+      AT sum = ev[(uint32_t)sorted[t]];
+      for (int t2 = t + 1; t2 < nn && (uint32_t)(sorted[t2] >> 32) == key; ++t2) sum += ev[(uint32_t)sorted[t2]];
+      const int64_t pos = carry + ex;
+      if (pos < nz) {
+        ccol[c0 + pos] = (int32_t)key;
+        cval[c0 + pos] = sum;
+      }
+    }
+    carry += tot;
+  }
+  if (threadIdx.x == 0 && carry != nz) dev_report(st, carry > nz ? kDevRowOverflow : kDevRowUnderflow, 11, r);
+}
+
+// Hash accumulator for rows with at most 2^TBITS / 2 distinct columns: linear
+// probing on 32-bit keys with the value summed by shared-memory atomics
+// (ams_hash_numc_krnl, src/ams/ams_utils.c:238-296, in shared memory), then
+// the occupied slots are compacted, sorted by column, and written in order.
+template <int BLOCK, int TBITS, typename VIn>
+__global__ void __launch_bounds__(BLOCK)
+k_numc_hash(const int32_t* __restrict__ rows, Csr A, Csr B, const int64_t* __restrict__ crp,
+            int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval, DevStatus* st) {
+  using AT = typename Acc<VIn>::T;
+  constexpr int T = 1 << TBITS;
+  constexpr int NCAP = T / 2;
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint32_t* tkey = reinterpret_cast<uint32_t*>(smem);         // T keys; later NCAP sort items
+  AT* tval = reinterpret_cast<AT*>(smem + T * sizeof(uint32_t));
+  uint64_t* items = reinterpret_cast<uint64_t*>(tval + T);     // NCAP compacted items
+  SortScratch<BLOCK>& ss = *reinterpret_cast<SortScratch<BLOCK>*>(items + NCAP);
+  Stage<VIn>& sg = *reinterpret_cast<Stage<VIn>*>(reinterpret_cast<uint8_t*>(&ss) + sizeof(SortScratch<BLOCK>));
+  __shared__ uint32_t s_min, s_max;
+  __shared__ int s_cnt, s_full;
+  const int64_t r = rows[blockIdx.x];
+  for (int i = threadIdx.x; i < T; i += BLOCK) {
+    tkey[i] = kEmptyKey;
+    tval[i] = AT(0);
+  }
+  if (threadIdx.x == 0) { s_min = 0xFFFFFFFFu; s_max = 0u; s_cnt = 0; s_full = 0; }
+  __syncthreads();
+  bool full = false;
+  expand_row<BLOCK, true, VIn>(A, B, r, sg, false, 0, 0, [&](int32_t key, VIn av, VIn bv, int64_t) {
+    const AT v = Acc<VIn>::mul(av, bv);
+    uint32_t h = hash_slot((uint32_t)key, TBITS);
+    for (int probe = 0; probe < T; ++probe) {
+      const uint32_t cur = tkey[h];
+      if (cur == (uint32_t)key) { Acc<VIn>::atomic_add(&tval[h], v); return; }
+      if (cur == kEmptyKey) {
+        const uint32_t old = atomicCAS(&tkey[h], kEmptyKey, (uint32_t)key);
+        if (old == kEmptyKey || old == (uint32_t)key) { Acc<VIn>::atomic_add(&tval[h], v); return; }
+      }
+      h = (h + 1) & (T - 1);
+    }
+    full = true;
+  });
+  if (full) s_full = 1;
+  __syncthreads();
+  // compact occupied slots into items (warp-aggregated slot reservation)
+  const int lane = threadIdx.x & 31;
+  uint32_t kmin = 0xFFFFFFFFu, kmax = 0u;
+  for (int i0 = 0; i0 < T; i0 += BLOCK) {
+    const int i = i0 + threadIdx.x;
+    const uint32_t k = i < T ? tkey[i] : kEmptyKey;
+    const bool occ = k != kEmptyKey;
+    const unsigned m = __ballot_sync(kFull, occ);
+    int base = 0;
+    if (lane == 0 && m) base = atomicAdd(&s_cnt, __popc(m));
+    base = __shfl_sync(kFull, base, 0);
+    if (occ) {
+      const int pos = base + __popc(m & lanemask_lt());
+      if (pos < NCAP) items[pos] = ((uint64_t)k << 32) | (uint64_t)i;
+      kmin = min(kmin, k);
+      kmax = max(kmax, k);
+    }
+  }
+  kmin = warp_min_u32(kmin);
+  kmax = warp_max_u32(kmax);
+  if (lane == 0) {
+    atomicMin(&s_min, kmin);
+    atomicMax(&s_max, kmax);
+  }
+  __syncthreads();
+  const int64_t c0 = crp[r], nz = crp[r + 1] - c0;
+  const int n = s_cnt;
+  if (s_full || n > NCAP) {
+    if (threadIdx.x == 0) dev_report(st, kDevTableFull, 12, r);
+    return;
+  }
+  uint64_t* spare = reinterpret_cast<uint64_t*>(tkey);  // keys are no longer needed
+  const uint64_t* sorted = block_radix_sort<BLOCK>(items, spare, n, s_min, s_max, ss.hist, ss.tmp);
+  for (int t = threadIdx.x; t < n && t < nz; t += BLOCK) {
+    const uint64_t it = sorted[t];
+    ccol[c0 + t] = (int32_t)(it >> 32);
+    cval[c0 + t] = tval[(uint32_t)it];
+  }
+  if (threadIdx.x == 0 && n != nz) dev_report(st, n > nz ? kDevRowOverflow : kDevRowUnderflow, 12, r);
+}
+
+// Heavy rows: dense accumulation over kDenseChunkCols columns at a time
+// (values plus a presence bitmap in shared memory), written in column order
+// straight from the chunk, so no sort is needed.  B rows are cut to each
+// chunk by binary search (B rows sorted by column).
+template <int BLOCK, typename VIn>
+__global__ void __launch_bounds__(BLOCK)
+k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, const int64_t* __restrict__ crp,
+             int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval, DevStatus* st) {
+  using AT = typename Acc<VIn>::T;
+  constexpr int CW = kDenseChunkCols;
+  constexpr int NWORD = CW / 32;
+  static_assert(NWORD <= BLOCK, "one bitmap word per thread");
+  extern __shared__ __align__(16) uint8_t smem[];
+  AT* dv = reinterpret_cast<AT*>(smem);
+  uint32_t* bm = reinterpret_cast<uint32_t*>(dv + CW);
+  Stage<VIn>& sg = *reinterpret_cast<Stage<VIn>*>(reinterpret_cast<uint8_t*>(bm + NWORD));
+  const int64_t r = rows[blockIdx.x];
+  const int64_t c0r = crp[r], nz = crp[r + 1] - c0r;
+  const bool multi = c_ncol > CW;
+  int64_t written = 0;
+  for (int64_t c0 = 0; c0 < c_ncol; c0 += CW) {
+    const int64_t c1 = (c_ncol < c0 + CW ? c_ncol : c0 + CW);
+    for (int i = threadIdx.x; i < CW; i += BLOCK) dv[i] = AT(0);
+    for (int i = threadIdx.x; i < NWORD; i += BLOCK) bm[i] = 0u;
+    __syncthreads();
+    expand_row<BLOCK, true, VIn>(A, B, r, sg, multi, (int32_t)c0, (int32_t)c1,
+                                 [&](int32_t key, VIn av, VIn bv, int64_t) {
+      const int64_t idx = (int64_t)key - c0;
+      if (idx < 0 || idx >= CW) return;
+      atomicOr(&bm[idx >> 5], 1u << (idx & 31));
+      Acc<VIn>::atomic_add(&dv[idx], Acc<VIn>::mul(av, bv));
+    });
+    __syncthreads();
+    uint32_t word = threadIdx.x < NWORD ? bm[threadIdx.x] : 0u;
+    long long tot;
+    const long long ex = block_exclusive_sum<BLOCK, long long>((long long)__popc(word), sg.tmp, tot);
+    int64_t pos = written + ex;
+    while (word) {
+      const int b = __ffs(word) - 1;
+      word &= word - 1;
+      if (pos < nz) {
+        ccol[c0r + pos] = (int32_t)(c0 + threadIdx.x * 32 + b);
+        cval[c0r + pos] = dv[threadIdx.x * 32 + b];
+      }
+      ++pos;
+    }
+    written += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && written != nz) dev_report(st, written > nz ? kDevRowOverflow : kDevRowUnderflow, 13, r);
+}
+
+}  // namespace cas

@@ -1,0 +1,95 @@
+// casgemm kernels for C = A * B on sm_100a (B = A^T in every benchmark
+// configuration, but B is read as its own CSR, as in the reference).
+//
+// CSR layout in HBM: int64 row pointers, int32 column indices, values fp64
+// (or int32 in / int64 out for the integer mode).  Every row of C is written
+// with its columns sorted.
+//
+// Pipeline (the reference's four phases, src/ams_hybaccspgemm.c:36-215):
+//   INIT  k_flp            row_flp[i] = sum_{k in A_i} |B_k|   (flp_populate,
+//                          src/mm/mm_utils.c:1063-1125), total products
+//         k_bin_*          rows binned by intermediate-product count: the
+//                          GPU form of the morsel packing of pack_ams_pack
+//                          (src/ams/ams_utils.c:1410-1596)
+//   SYMB  k_symb_*         exact distinct-column count per row
+//                          (ams_hash_symb_dnr, src/ams/ams_utils.c:1630-1752)
+//         k_scan_*         exclusive scan -> C row pointers (scan,
+//                          src/mm/mm_utils.c:866-957)
+//   NUMC  k_numc_*         hash / ESC / hybrid accumulation
+//                          (src/ams/ams_utils.c:168-475, 956-1338)
+#pragma once
+#include "cas_device.cuh"
+
+namespace cas {
+
+// ------------------------------------------------------------ parameters
+// Symbolic bins by t = min(row_flp, num_col) (an upper bound on the row's
+// distinct columns); numeric bins by accumulator and size.
+enum SymbBin : int {
+  kSB_Zero = 0,    // row_flp == 0
+  kSB_Tiny = 1,    // row_flp <= 32: one warp, one product per lane
+  kSB_H512 = 2,    // t <= 256:   128 threads, 512-slot table
+  kSB_H2K = 3,     // t <= 1024:  256 threads, 2048-slot table
+  kSB_H8K = 4,     // t <= 4096:  512 threads, 8192-slot table
+  kSB_H32K = 5,    // t <= 16384: 1024 threads, 32768-slot table
+  kSB_Dense = 6,   // larger: column bitmap in shared memory
+  kSymbBins = 7
+};
+
+enum NumcBin : int {
+  kNB_Zero = 0,    // no products
+  kNB_Tiny = 1,    // row_flp <= 32: warp sort in registers
+  kNB_E1K = 2,     // ESC, row_flp <= 1024 (256 threads)
+  kNB_E2K = 3,     // ESC, row_flp <= 2048 (256 threads)
+  kNB_E4K = 4,     // ESC, row_flp <= 4096 (512 threads)
+  kNB_E8K = 5,     // ESC, row_flp <= 8192 (1024 threads)
+  kNB_H256 = 6,    // hash, nnz <= 256   (128 threads, 512 slots)
+  kNB_H1K = 7,     // hash, nnz <= 1024  (256 threads, 2048 slots)
+  kNB_H4K = 8,     // hash, nnz <= 4096  (512 threads, 8192 slots)
+  kNB_Dense = 9,   // dense column chunks in shared memory
+  kNumcBins = 10
+};
+
+enum AccumMode : int { kAccHash = 0, kAccEsc = 1, kAccHybrid = 2 };
+
+constexpr int kDenseChunkBits = 1 << 20;   // symbolic bitmap chunk: 1 Mi columns (128 KiB)
+constexpr int kDenseChunkCols = 16384;     // numeric dense chunk: 16 Ki columns (128 KiB of values)
+
+struct Csr {
+  int64_t nrow, ncol;
+  const int64_t* __restrict__ rp;
+  const int32_t* __restrict__ col;
+  const void* __restrict__ val;
+};
+
+__host__ __device__ __forceinline__ int symb_bin_of(int64_t flp, int64_t ncol) {
+  if (flp <= 0) return kSB_Zero;
+  if (flp <= 32) return kSB_Tiny;
+  const int64_t t = flp < ncol ? flp : ncol;
+  if (t <= 256) return kSB_H512;
+  if (t <= 1024) return kSB_H2K;
+  if (t <= 4096) return kSB_H8K;
+  if (t <= 16384) return kSB_H32K;
+  return kSB_Dense;
+}
+
+// Accumulator choice of one row: the hybrid mode takes ESC when the row's
+// compression factor flp/nnz is below the threshold, as
+// ams_hybacc_numc_krnl does (src/ams/ams_utils.c:1139-1149).
+__host__ __device__ __forceinline__ int numc_bin_of(int64_t flp, int64_t nz, int mode, double thres) {
+  if (flp <= 0 || nz <= 0) return kNB_Zero;
+  if (flp <= 32) return kNB_Tiny;
+  bool esc = mode == kAccEsc || (mode == kAccHybrid && (double)flp / (double)nz < thres);
+  if (esc) {
+    if (flp <= 1024) return kNB_E1K;
+    if (flp <= 2048) return kNB_E2K;
+    if (flp <= 4096) return kNB_E4K;
+    if (flp <= 8192) return kNB_E8K;
+  }
+  if (nz <= 256) return kNB_H256;
+  if (nz <= 1024) return kNB_H1K;
+  if (nz <= 4096) return kNB_H4K;
+  return kNB_Dense;
+}
+
+}  // namespace cas

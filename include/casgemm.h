@@ -1,0 +1,151 @@
+/*
+ * casgemm — C = A·B sparse-sparse product on one NVIDIA B200 (sm_100a), the
+ * drop-in for the CPU SpGEMM of fukien/contention-aware-spgemm (C = A·Aᵀ with
+ * B = Aᵀ read as its own CSR, as the reference's drivers do).
+ *
+ * Plain C ABI: pointers, sizes, status codes; no C++ or torch types.
+ * Every function returns a cas_status; on failure cas_last_error() describes
+ * it.  A context is bound to one device and one CUDA stream and is not
+ * re-entrant (the reference is not either: it keeps process-global state,
+ * src/ams/ams_utils.c:29-33); use one context per host thread.
+ *
+ * Output: every row of C has its columns sorted ascending, and each value is
+ * the sum of its products.  The reference's hash accumulator leaves rows in
+ * hash-slot order (src/ams/ams_utils.c:301-309); sorted rows are the same set
+ * of (row, col, value) entries.
+ */
+#ifndef CASGEMM_H
+#define CASGEMM_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+	CAS_OK = 0,
+	CAS_ERR_BAD_INPUT = 1,   /* shapes, pointers or index widths are invalid */
+	CAS_ERR_OOM = 2,         /* device or host allocation failed */
+	CAS_ERR_CUDA = 3,        /* a CUDA call failed */
+	CAS_ERR_DEVICE = 4,      /* a device-side guard fired (see cas_last_error) */
+	CAS_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
+	CAS_ERR_ABORTED = 6,     /* cancelled by the caller */
+	CAS_ERR_REJECTED = 7     /* a request that can never fit the memory budget */
+} cas_status;
+
+/* The three accumulators of the reference's drivers. */
+typedef enum {
+	CAS_ACC_HASH = 0,    /* ams_hashspgemm   (ams_hash_numc,   src/ams/ams_utils.c:608)  */
+	CAS_ACC_HSERSC = 1,  /* ams_hserscspgemm (ams_hsersc_numc, src/ams/ams_utils.c:781)  */
+	CAS_ACC_HYBACC = 2   /* ams_hybaccspgemm (ams_hybacc_numc, src/ams/ams_utils.c:1159) */
+} cas_accum;
+
+/* Value arithmetic. */
+typedef enum {
+	CAS_VAL_F64 = 0,     /* fp64 in, fp64 out (the reference's my_rat_t, src/inc/store.h:20) */
+	CAS_VAL_I32 = 1      /* int32 in, int64 out (exact integer accumulation) */
+} cas_valtype;
+
+/* CSR matrix.  Layout-compatible with the reference's csr_t
+ * (src/inc/store.h:49-56) when col_bytes == 8, val_type == CAS_VAL_F64 and
+ * on_device == 0: the first six fields line up. */
+typedef struct {
+	int64_t num_row;
+	int64_t num_col;
+	int64_t num_nnz;
+	int64_t *row_ptrs;   /* num_row + 1 entries */
+	void *cols;          /* int32 (col_bytes 4) or int64 (col_bytes 8) column indices */
+	void *rats;          /* values: double, or int32 input / int64 output for CAS_VAL_I32 */
+	int32_t col_bytes;   /* 4 or 8; device matrices use 4 */
+	int32_t val_type;    /* cas_valtype */
+	int32_t on_device;   /* 1: pointers are device memory of the context's device */
+	int32_t owned;       /* set by the library when it allocated the arrays; see cas_csr_free */
+} cas_csr;
+
+/* Phase times in seconds, the reference's runtime_t (src/mm/mm_utils.h:48-54);
+ * measured with CUDA events on the context's stream. */
+typedef struct {
+	double init_time;
+	double symb_time;
+	double mgmt_time;
+	double numc_time;
+	double total_time;
+} cas_runtime;
+
+#define CAS_SYMB_BINS 7
+#define CAS_NUMC_BINS 10
+
+/* Counters of the last cas_spgemm call. */
+typedef struct {
+	int64_t flop;                          /* intermediate products (flop_cnt, get_intprod) */
+	int64_t max_row_flp;                   /* largest row product count */
+	int64_t nnz_c;
+	int64_t symb_bin_rows[CAS_SYMB_BINS];  /* rows per symbolic bin */
+	int64_t numc_bin_rows[CAS_NUMC_BINS];  /* rows per numeric bin */
+	int64_t kernel_launches;               /* kernels launched by the library since cas_create */
+	double h2d_bytes;                      /* host->device bytes copied by the call */
+	double d2h_bytes;                      /* device->host bytes copied by the call */
+} cas_stats;
+
+typedef struct cas_ctx cas_ctx;
+
+/* Context on `device`; the stream is a new non-blocking stream. */
+cas_status cas_create(int device, cas_ctx **out);
+void cas_destroy(cas_ctx *ctx);
+/* Use an existing cudaStream_t (passed as void*); NULL restores the context's own. */
+cas_status cas_set_stream(cas_ctx *ctx, void *stream);
+/* AMS_ACC_THRES of the hybrid accumulator (cmake/Options.cmake:142-146):
+ * rows with products/nnz below it take ESC.  Default 2.0, the R-MAT run
+ * script's value for ams_hybaccspgemm (scripts/ams_rmat_run.sh:33). */
+cas_status cas_set_acc_thres(cas_ctx *ctx, double thres);
+const char *cas_last_error(const cas_ctx *ctx);
+cas_status cas_get_stats(const cas_ctx *ctx, cas_stats *out);
+
+/* ---- the reference's phase functions, on device CSR (col_bytes 4) ------ */
+
+/* row_flp[i] = sum over A_i of |B_k| into device memory (m entries).
+ * Replaces flp_populate (src/mm/mm_utils.c:1089-1125). */
+cas_status cas_flp_populate(cas_ctx *ctx, const cas_csr *A, const cas_csr *B, int64_t *d_row_flp);
+
+/* d_out[0] = 0, d_out[i+1] = d_out[i] + d_in[i] for i < n-1 (device arrays).
+ * Replaces scan (src/mm/mm_utils.c:903-957). */
+cas_status cas_scan(cas_ctx *ctx, int64_t *d_out, const int64_t *d_in, int64_t n);
+
+/* Exact distinct-column count of every row of A·B into d_row_nz (m entries),
+ * given d_row_flp from cas_flp_populate.  Replaces ams_hash_symb_dnr
+ * (src/ams/ams_utils.c:1701-1752) and ams_hash_symb (:483-602). */
+cas_status cas_hash_symb(cas_ctx *ctx, const cas_csr *A, const cas_csr *B, const int64_t *d_row_flp,
+	int64_t *d_row_nz);
+
+/* Numeric phase into a caller-allocated device C whose row_ptrs are the scan
+ * of the symbolic counts (C->num_nnz entries of cols/rats).
+ * Replace ams_hash_numc (src/ams/ams_utils.c:608-774), ams_hsersc_numc
+ * (:781-949) and ams_hybacc_numc (:1159-1338). */
+cas_status cas_hash_numc(cas_ctx *ctx, const cas_csr *A, const cas_csr *B, const int64_t *d_row_flp,
+	cas_csr *C);
+cas_status cas_hsersc_numc(cas_ctx *ctx, const cas_csr *A, const cas_csr *B, const int64_t *d_row_flp,
+	cas_csr *C);
+cas_status cas_hybacc_numc(cas_ctx *ctx, const cas_csr *A, const cas_csr *B, const int64_t *d_row_flp,
+	cas_csr *C);
+
+/* ---- whole product --------------------------------------------------- */
+
+/* C = A·B with the given accumulator: the four phases of the drivers'
+ * hashspgemm / hserscspgemm / hybaccspgemm (src/ams_hashspgemm.c:36-205,
+ * src/ams_hserscspgemm.c:36-210, src/ams_hybaccspgemm.c:36-215).
+ * A and B may be host (either column width) or device (col_bytes 4) CSR.
+ * C is allocated by the library: on the device when C->on_device is 1 on
+ * entry (col_bytes 4), else in host memory with C->col_bytes (4 or 8) columns.
+ * C->val_type is CAS_VAL_F64 for fp64 inputs and CAS_VAL_I32 (int64 values)
+ * for int32 inputs.  Release C with cas_csr_free.  rt may be NULL. */
+cas_status cas_spgemm(cas_ctx *ctx, cas_accum accum, const cas_csr *A, const cas_csr *B, cas_csr *C,
+	cas_runtime *rt);
+
+/* Frees arrays the library allocated (owned != 0) and zeroes the struct. */
+cas_status cas_csr_free(cas_ctx *ctx, cas_csr *C);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

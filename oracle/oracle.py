@@ -1,0 +1,170 @@
+"""TEST INFRASTRUCTURE — ctypes access to the two CPU oracles.
+
+* :func:`oracle_spgemm` — the project's C restatement (oracle/cas_oracle.c,
+  liboracle_cas.so) of the reference's algorithm.
+* :func:`ref_spgemm` — the reference itself (fukien/contention-aware-spgemm),
+  compiled from its unmodified sources into oracle/_ref/libref_<algo>.so with
+  a direct-call harness (oracle/ref_harness.c).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, and only to check or time the GPU product against; the product never
+imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liboracle_cas.so")
+REF_DIR = os.path.join(HERE, "_ref")
+ALGOS = {"hash": 0, "hsersc": 1, "hybacc": 2}
+# AMS_ACC_THRES of each reference build (scripts/ams_rmat_run.sh:25-36)
+REF_ACC_THRES = {"hash": 5.0, "hsersc": 5.0, "hybacc": 2.0}
+
+
+class OrcCsr(ctypes.Structure):
+    """The reference's csr_t (src/inc/store.h:49-56): int64 indices, fp64 values."""
+    _fields_ = [
+        ("num_row", ctypes.c_int64), ("num_col", ctypes.c_int64), ("num_nnz", ctypes.c_int64),
+        ("row_ptrs", ctypes.c_void_p), ("cols", ctypes.c_void_p), ("rats", ctypes.c_void_p),
+    ]
+
+
+class RefRuntime(ctypes.Structure):
+    """runtime_t (src/mm/mm_utils.h:48-54)."""
+    _fields_ = [(n, ctypes.c_double) for n in ("init_time", "symb_time", "mgmt_time", "numc_time", "total_time")]
+
+
+_orc = None
+_refs = {}
+
+
+def _load_oracle():
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORACLE_LIB):
+            raise FileNotFoundError(f"{ORACLE_LIB} missing: run `make -C {HERE}`")
+        lib = ctypes.CDLL(ORACLE_LIB)
+        P = ctypes.c_void_p
+        lib.orc_spgemm.restype = ctypes.c_int64
+        lib.orc_spgemm.argtypes = [ctypes.POINTER(OrcCsr), ctypes.POINTER(OrcCsr), ctypes.POINTER(OrcCsr),
+                                   ctypes.c_int, ctypes.c_double, ctypes.c_int]
+        lib.orc_free.argtypes = [ctypes.POINTER(OrcCsr)]
+        lib.orc_sort_rows.argtypes = [ctypes.POINTER(OrcCsr)]
+        lib.orc_flp_populate.argtypes = [ctypes.POINTER(OrcCsr), ctypes.POINTER(OrcCsr), P]
+        lib.orc_hash_symb.argtypes = [ctypes.POINTER(OrcCsr), ctypes.POINTER(OrcCsr), P, P]
+        lib.orc_scan.argtypes = [P, P, ctypes.c_int64]
+        lib.orc_intprod.restype = ctypes.c_int64
+        lib.orc_intprod.argtypes = [ctypes.POINTER(OrcCsr), ctypes.POINTER(OrcCsr)]
+        lib.orc_next_pow2.restype = ctypes.c_int64
+        lib.orc_next_pow2.argtypes = [ctypes.c_int64]
+        lib.orc_radix_sort_kv.argtypes = [P, P, P, P, ctypes.c_int64]
+        lib.orc_pack_morsels.restype = ctypes.c_int64
+        lib.orc_pack_morsels.argtypes = [ctypes.c_int64, P, P, P, ctypes.c_int64, ctypes.c_double, P, P, P, P,
+                                         ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+        _orc = lib
+    return _orc
+
+
+def _load_ref(algo: str, small: bool):
+    key = (algo, small)
+    if key not in _refs:
+        path = os.path.join(REF_DIR, f"libref_{algo}{'_small' if small else ''}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C {HERE} ref` where the reference sources exist")
+        lib = ctypes.CDLL(path)
+        lib.ref_spgemm.restype = ctypes.c_int
+        lib.ref_spgemm.argtypes = [ctypes.POINTER(OrcCsr)] * 3 + [ctypes.POINTER(RefRuntime)]
+        lib.ref_free_csr.argtypes = [ctypes.POINTER(OrcCsr)]
+        lib.ref_intprod.restype = ctypes.c_long
+        lib.ref_intprod.argtypes = [ctypes.POINTER(OrcCsr), ctypes.POINTER(OrcCsr)]
+        lib.ref_morsel_size.restype = ctypes.c_long
+        lib.ref_thread_num.restype = ctypes.c_int
+        lib.ref_acc_thres.restype = ctypes.c_double
+        _refs[key] = lib
+    return _refs[key]
+
+
+def ref_available(algo: str = "hybacc", small: bool = True) -> bool:
+    return os.path.exists(os.path.join(REF_DIR, f"libref_{algo}{'_small' if small else ''}.so"))
+
+
+def to_orc(rp, cols, vals, num_col) -> Tuple[OrcCsr, tuple]:
+    """Build a csr_t view (int64 columns, fp64 values); returns (struct, keep-alive)."""
+    rp = np.ascontiguousarray(rp, dtype=np.int64)
+    cols = np.ascontiguousarray(cols, dtype=np.int64)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    s = OrcCsr(len(rp) - 1, num_col, int(rp[-1]) if len(rp) else 0, rp.ctypes.data, cols.ctypes.data,
+               vals.ctypes.data)
+    return s, (rp, cols, vals)
+
+
+def _from_orc(c: OrcCsr):
+    m, nnz = c.num_row, c.num_nnz
+    rp = np.ctypeslib.as_array(ctypes.cast(c.row_ptrs, ctypes.POINTER(ctypes.c_int64)), (m + 1,)).copy()
+    if nnz > 0:
+        cols = np.ctypeslib.as_array(ctypes.cast(c.cols, ctypes.POINTER(ctypes.c_int64)), (nnz,)).copy()
+        vals = np.ctypeslib.as_array(ctypes.cast(c.rats, ctypes.POINTER(ctypes.c_double)), (nnz,)).copy()
+    else:
+        cols, vals = np.zeros(0, np.int64), np.zeros(0, np.float64)
+    return rp, cols, vals
+
+
+def sort_rows(rp, cols, vals):
+    """Canonical per-row column order (the hash accumulators emit slot order)."""
+    rows = np.repeat(np.arange(len(rp) - 1, dtype=np.int64), np.diff(rp))
+    order = np.lexsort((cols, rows))
+    return rp, cols[order], vals[order]
+
+
+def oracle_spgemm(A, B, algo: str = "hybacc", acc_thres: Optional[float] = None, sort: bool = True):
+    """C = A*B by the C restatement.  A, B: objects with num_row/num_col/row_ptrs/cols/vals.
+
+    Returns (row_ptrs, cols int64, vals f64, flop)."""
+    lib = _load_oracle()
+    a, ka = to_orc(A.row_ptrs, A.cols, A.vals, A.num_col)
+    b, kb = to_orc(B.row_ptrs, B.cols, B.vals, B.num_col)
+    c = OrcCsr()
+    thres = REF_ACC_THRES[algo] if acc_thres is None else acc_thres
+    flop = lib.orc_spgemm(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ALGOS[algo], thres, int(sort))
+    try:
+        rp, cols, vals = _from_orc(c)
+    finally:
+        lib.orc_free(ctypes.byref(c))
+    del ka, kb
+    return rp, cols, vals, int(flop)
+
+
+def ref_spgemm(A, B, algo: str = "hybacc", small: bool = True):
+    """C = A*B by the reference's own kernels; rows sorted for comparison.
+
+    Returns (row_ptrs, cols, vals, runtime dict) or None when the input is
+    below one morsel (the reference would exit(1))."""
+    lib = _load_ref(algo, small)
+    a, ka = to_orc(A.row_ptrs, A.cols, A.vals, A.num_col)
+    b, kb = to_orc(B.row_ptrs, B.cols, B.vals, B.num_col)
+    c = OrcCsr()
+    rt = RefRuntime()
+    st = lib.ref_spgemm(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(rt))
+    if st != 0:
+        return None
+    try:
+        rp, cols, vals = _from_orc(c)
+    finally:
+        lib.ref_free_csr(ctypes.byref(c))
+    del ka, kb
+    rp, cols, vals = sort_rows(rp, cols, vals)
+    return rp, cols, vals, {n: getattr(rt, n) for n, _ in RefRuntime._fields_}
+
+
+def ref_info(algo: str = "hybacc", small: bool = False) -> dict:
+    lib = _load_ref(algo, small)
+    return {"threads": lib.ref_thread_num(), "morsel": lib.ref_morsel_size(), "acc_thres": lib.ref_acc_thres()}
+
+
+def oracle_lib():
+    return _load_oracle()

@@ -1,0 +1,72 @@
+"""GPU parity: casgemm (CUDA, through the C ABI) against the CPU oracle.
+
+Integer-valued products must match bit for bit (row pointers, sorted column
+indices, values).  The one case with real-valued inputs is compared with
+rtol 1e-12: fp64 sums in a different order round differently.
+"""
+import numpy as np
+import pytest
+
+import casgemm
+import oracle
+from matrices import cases, with_int_values
+
+pytestmark = pytest.mark.gpu
+
+CASES = cases()
+IDS = [c[0] for c in CASES]
+
+
+def check(res: casgemm.Csr, ref, exact: bool, name: str):
+    rp, cols, vals = ref[0], ref[1], ref[2]
+    assert np.array_equal(res.row_ptrs, rp), f"{name}: row pointers differ"
+    assert np.array_equal(res.cols.astype(np.int64), cols), f"{name}: columns differ"
+    if exact:
+        assert np.array_equal(res.vals.astype(np.float64), vals), f"{name}: values differ"
+    else:
+        np.testing.assert_allclose(res.vals, vals, rtol=1e-12, atol=1e-12 * max(1.0, float(np.abs(vals).max())))
+
+
+@pytest.mark.parametrize("algo", ["hash", "hsersc", "hybacc"])
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_f64(ctx, case, algo):
+    name, A, B = case
+    ref = oracle.oracle_spgemm(A, B, algo)
+    out = ctx.spgemm(A, B, algo)
+    exact = name != "general_AB"
+    check(out.csr, ref, exact, name)
+    assert out.stats["flop"] == ref[3]
+    assert out.stats["nnz_c"] == len(ref[1])
+
+
+@pytest.mark.parametrize("algo", ["hash", "hybacc"])
+@pytest.mark.parametrize("case", CASES[:8], ids=IDS[:8])
+def test_int32_values(ctx, case, algo):
+    """int32 values 1..8 in, int64 sums out (the batched configuration's arithmetic)."""
+    name, A, _ = case
+    Ai = with_int_values(A, 41)
+    Bi = Ai.transpose()
+    ref = oracle.oracle_spgemm(Ai, Bi, algo)
+    out = ctx.spgemm(Ai, Bi, algo)
+    assert out.csr.vals.dtype == np.int64
+    check(out.csr, ref, True, name)
+
+
+def test_reference_layout_int64_columns(ctx):
+    """A csr_t-shaped input (int64 columns, src/inc/store.h:49-56) and int64 output columns."""
+    A = casgemm.gen_g500(10, 8, 3)
+    T = A.transpose()
+    A64 = casgemm.Csr(A.num_row, A.num_col, A.row_ptrs, A.cols.astype(np.int64), A.vals)
+    B64 = casgemm.Csr(T.num_row, T.num_col, T.row_ptrs, T.cols.astype(np.int64), T.vals)
+    out = ctx.spgemm(A64, B64, "hybacc", col_bytes=8)
+    ref = oracle.oracle_spgemm(A, T, "hybacc")
+    assert out.csr.cols.dtype == np.int64
+    check(out.csr, ref, True, "int64 columns")
+
+
+def test_runtime_phases(ctx):
+    A = casgemm.gen_g500(12, 8, 9)
+    out = ctx.spgemm(A, A.transpose(), "hybacc")
+    rt = out.runtime
+    assert all(rt[k] >= 0 for k in rt)
+    assert abs(rt["total_time"] - (rt["init_time"] + rt["symb_time"] + rt["mgmt_time"] + rt["numc_time"])) < 1e-9
