@@ -1,0 +1,422 @@
+#!/usr/bin/env python
+"""Benchmark of the casgemm C = A·Aᵀ SpGEMM on B200 (one JSON line on stdout).
+
+Workload (default): the uniform (ER) R-MAT graph of scale 21, edge factor 32
+(2,097,152 vertices, 67,108,864 undirected edges, a=b=c=d=0.25, seed 21),
+symmetrised, loop- and duplicate-free, values 1.0 (fp64), int32 columns; C =
+A·Aᵀ with B = Aᵀ as its own CSR, hybrid accumulator.  The largest
+single-matrix configuration that fits one B200 (C alone is about 103 GB).
+
+One step = one full product — the four phases of the reference's drivers
+(flop count, symbolic, allocation, numeric) plus freeing C — with A and B
+resident in HBM.  `value` = 2 * intermediate products / step time, in
+GFLOP/s.  Timed with CUDA events on the launching stream, max over ranks.
+The inputs (1.6 GB each) are far larger than the 126 MB L2, so L2 is not
+flushed between steps.
+
+`--impl reference` times the reference's own CPU code (built from its sources
+into oracle/_ref) on a bounded row sample of the same matrix on the host's
+cores.  Under torchrun only rank 0 runs it.
+
+Multi-GPU (torchrun, one rank per GPU): the rows of A are split into
+contiguous shards of equal products; each rank computes its shard of C with
+B replicated; no data-path collective (scaling: strong, total work fixed).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "contention-aware-spgemm_b200"))
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    # name: (family, scale, edge_factor, seed)
+    "er_s21_ef32": ("er", 21, 32, 21),
+    "g500_s17_ef8": ("g500", 17, 8, 17),
+    "er_s18_ef32": ("er", 18, 32, 18),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_matrix(name):
+    import casgemm
+    fam, s, ef, seed = WORKLOADS[name]
+    A = casgemm.gen_er(s, ef, seed) if fam == "er" else casgemm.gen_g500(s, ef, seed)
+    return A
+
+
+def row_products(A, B):
+    """Prefix of intermediate products over the rows of A (length num_row + 1)."""
+    cnt = np.diff(B.row_ptrs)[A.cols].astype(np.int64)
+    return np.concatenate([[0], np.cumsum(cnt)])[A.row_ptrs]
+
+
+def row_shard(A, B, rank, world, r_end):
+    """Contiguous rows [r0, r1) of [0, r_end) holding about 1/world of their products."""
+    if world == 1:
+        return 0, r_end
+    ps = row_products(A, B)[: r_end + 1]
+    total = int(ps[-1])
+    r0 = int(np.searchsorted(ps, total * rank // world, side="left"))
+    r1 = int(np.searchsorted(ps, total * (rank + 1) // world, side="left")) if rank + 1 < world else r_end
+    return r0, r1
+
+
+def slice_rows(A, r0, r1):
+    import casgemm
+    s, e = int(A.row_ptrs[r0]), int(A.row_ptrs[r1])
+    return casgemm.Csr(r1 - r0, A.num_col, A.row_ptrs[r0:r1 + 1] - s, A.cols[s:e], A.vals[s:e])
+
+
+def sample_rows_for(A, B, target_products):
+    """Rows [0, R) whose products reach target_products (a bounded CPU sample)."""
+    ps = row_products(A, B)
+    R = int(np.searchsorted(ps, target_products, side="left"))
+    R = max(1, min(R, A.num_row))
+    return R, int(ps[R])
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.gpu = str(gpu_index)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", self.gpu], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def gpu_index(local_rank):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [x for x in vis.split(",") if x.strip()]
+        if local_rank < len(ids):
+            return ids[local_rank]
+    return local_rank
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic(kernel, workload):
+    """Per-launch DRAM traffic of `kernel` from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        e = d.get(kernel, {}).get(workload)
+        return None if e is None else float(e)
+    except Exception:
+        return None
+
+
+def cpu_reference(A, B, target_products, steps, warmup):
+    """The reference's hybrid driver on rows [0, R): per-step GFLOP/s (its own phase timer)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the reference built from its sources (oracle/_ref)
+    R, P = sample_rows_for(A, B, target_products)
+    As = slice_rows(A, 0, R)
+    times = []
+    for i in range(warmup + steps):
+        out = oracle.ref_spgemm(As, B, "hybacc", small=False)
+        if out is None:
+            raise RuntimeError("sample below one morsel")
+        if i >= warmup:
+            times.append(out[3]["total_time"])
+        del out
+    t = statistics.mean(times)
+    info = oracle.ref_info("hybacc", small=False)
+    return {"value": 2.0 * P / t / 1e9, "unit": "GFLOP/s", "cores": info["threads"], "kind": "reference",
+            "sample": f"rows [0,{R}) of {A.num_row}: {P} products ({100.0 * P / max(1, total_products(A, B)):.1f}% "
+                      f"of the workload), ams_hybaccspgemm kernels, {steps} runs after {warmup} warm-up, "
+                      f"mean total_time {t:.3f} s"}
+
+
+_TOTAL_P = {}
+
+
+def total_products(A, B):
+    key = id(A)
+    if key not in _TOTAL_P:
+        import casgemm
+        _TOTAL_P[key] = casgemm.intprod(A, B)
+    return _TOTAL_P[key]
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    A = make_matrix(args.workload)
+    B = A  # symmetric: Aᵀ has the same CSR
+    base = cpu_reference(A, B, args.ref_products, args.steps, args.warmup)
+    line = {"metric": "SpGEMM GFLOP/s (2 x intermediate products / s), C = A*A^T",
+            "value": base["value"], "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded R-MAT)", "impl": "reference",
+            "config": {"workload": args.workload, "accumulator": "hybacc", "sample": base["sample"]},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cas", choices=["cas", "reference"])
+    ap.add_argument("--workload", default="er_s21_ef32", choices=sorted(WORKLOADS))
+    ap.add_argument("--accum", default="hybacc", choices=["hash", "hsersc", "hybacc"])
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--ref-products", type=float, default=4e8,
+                    help="products in the CPU reference's row sample")
+    ap.add_argument("--row-fraction", type=float, default=1.0,
+                    help="use only the first fraction of A's rows (profiling captures; B stays whole)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+
+    import torch
+    import casgemm
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    t0 = time.time()
+    A = make_matrix(args.workload)
+    B = A  # Aᵀ of a symmetric matrix has the same CSR
+    r_end = max(1, int(round(A.num_row * args.row_fraction)))
+    r0, r1 = row_shard(A, B, rank, world, r_end)
+    As = slice_rows(A, r0, r1)
+    log(f"[rank {rank}] matrix {args.workload}: n={A.num_row} nnz={A.nnz} rows [{r0},{r1}) in {time.time() - t0:.1f}s")
+
+    def to_dev(M):
+        rp = torch.from_numpy(np.ascontiguousarray(M.row_ptrs)).to(dev)
+        c = torch.from_numpy(np.ascontiguousarray(M.cols)).to(dev)
+        v = torch.from_numpy(np.ascontiguousarray(M.vals)).to(dev)
+        return casgemm.DeviceCsr(M.num_row, M.num_col, M.nnz, rp.data_ptr(), c.data_ptr(), v.data_ptr(),
+                                 keep=(rp, c, v))
+
+    dA, dB = to_dev(As), to_dev(B)
+    ctx = casgemm.Context(dev.index)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+
+    def step():
+        cc, rt = ctx.spgemm_device(dA, dB, args.accum)
+        ctx.free(cc)
+        return rt
+
+    for _ in range(args.warmup):
+        step()
+    st_w = ctx.stats()
+    launches0 = st_w["kernel_launches"]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(gpu_index(local_rank))
+    sampler.start()
+    time.sleep(0.3)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    rts = []
+    for _ in range(args.steps):
+        rts.append(step())
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    if dist:
+        dist.barrier()
+    stats = ctx.stats()
+    launches = stats["kernel_launches"] - launches0
+    elapsed_ms = ev0.elapsed_time(ev1)
+    P_local = stats["flop"]
+    nnz_local = stats["nnz_c"]
+    if dist:
+        t = torch.tensor([elapsed_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+        tot = torch.tensor([P_local, nnz_local, launches], device=dev, dtype=torch.float64)
+        dist.all_reduce(tot)
+        P_total, nnz_total, launches_total = int(tot[0].item()), int(tot[1].item()), int(tot[2].item())
+    else:
+        P_total, nnz_total, launches_total = P_local, nnz_local, launches
+    ms_step = elapsed_ms / args.steps
+    value = 2.0 * P_total / (ms_step * 1e-3) / 1e9
+
+    # per-kernel times for the roofline: extra steps with the bins run one at
+    # a time and each bin kernel timed by CUDA events on its stream
+    ctx.set_profiling(True)
+    bin_ms, bin_bytes = {}, {}
+    n_prof = 2
+    ovf_rows, ovf_ms = 0, 0.0
+    for _ in range(n_prof):
+        step()
+        s = ctx.stats()
+        for k, v in s["numc_bin_ms"].items():
+            bin_ms[k] = bin_ms.get(k, 0.0) + v / n_prof
+            bin_bytes[k] = bin_bytes.get(k, 0.0) + s["numc_bin_bytes"][k] / n_prof
+        ovf_rows, ovf_ms = s["esc_overflow_rows"], ovf_ms + s["esc_overflow_ms"] / n_prof
+    ctx.set_profiling(False)
+
+    # roofline of the dominant kernel (the numeric bin with the most device time)
+    peak, peak_kind = measured_peak()
+    dom = max(bin_ms, key=lambda k: bin_ms[k])
+    dom_ms = bin_ms[dom]
+    dom_bytes = bin_bytes[dom]
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9 if dom_ms > 0 else 0.0
+    kernel_name = {"tiny": "k_numc_tiny<256>", "hash256": "k_numc_hash<256,9>", "hash1k": "k_numc_hash<256,11>",
+                   "hash4k": "k_numc_hash<512,13>", "dense": "k_numc_dense<1024>"}.get(dom)
+    if kernel_name is None and dom.startswith("esc"):
+        kernel_name = f"k_numc_esc_msd<256,{int(dom[3:-1]) * 1024}>"
+    alg_bytes_total = 12.0 * (A.nnz if world == 1 else As.nnz) + 12.0 * P_local + 12.0 * nnz_local + 16.0 * (As.num_row + 1)
+    pipe_frac = alg_bytes_total / (ms_step * 1e-3) / (peak * 1e9)
+
+    line = {
+        "metric": "SpGEMM GFLOP/s (2 x intermediate products / s), C = A*A^T",
+        "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded R-MAT, values 1.0)",
+        "config": {"workload": args.workload, "accumulator": args.accum, "row_fraction": args.row_fraction,
+                   "products": P_total, "nnz_c": nnz_total, "nnz_a": A.nnz, "n": A.num_row,
+                   "l2": "not flushed: inputs (1.6 GB each) exceed the 126 MB L2",
+                   "parallelism": f"row shards x{world}" if world > 1 else "1 GPU",
+                   "phases_ms_last_step": {k: round(v * 1e3, 3) for k, v in rts[-1].items()}},
+        "roofline": {"bound": "hbm", "kernel": kernel_name, "bin": dom,
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "alg_bytes_per_launch": dom_bytes, "launch_ms": round(dom_ms, 3),
+                     "timing": "CUDA events around the kernel, bins serialised, mean of 2 extra steps",
+                     "traffic": committed_traffic(kernel_name, args.workload)},
+        "numc_bins_ms": {k: round(v, 3) for k, v in bin_ms.items() if v > 0},
+        "esc_radix_fallback": {"rows": ovf_rows, "ms": round(ovf_ms, 3)},
+        "pipeline_roofline": {"alg_bytes": alg_bytes_total, "frac": round(pipe_frac, 4),
+                              "formula": "12*nnz(A)+12*P+12*nnz(C)+16*(m+1) over the step time"},
+        "gpu_launches": launches_total,
+        "clocks": clocks,
+    }
+
+    # end to end through the public C ABI with pinned host buffers: H2D of A and
+    # B, the product, D2H of C into host memory, every step
+    if not args.no_e2e:
+        pin = lambda x: torch.from_numpy(np.ascontiguousarray(x)).pin_memory()  # noqa: E731
+        hA = [pin(As.row_ptrs), pin(As.cols), pin(As.vals)]
+        hB = hA if (world == 1) else [pin(B.row_ptrs), pin(B.cols), pin(B.vals)]
+        ca = casgemm.CasCsr(As.num_row, As.num_col, As.nnz, hA[0].data_ptr(), hA[1].data_ptr(), hA[2].data_ptr(),
+                            4, 0, 0, 0)
+        cb = casgemm.CasCsr(B.num_row, B.num_col, B.nnz, hB[0].data_ptr(), hB[1].data_ptr(), hB[2].data_ptr(),
+                            4, 0, 0, 0)
+        import ctypes
+        walls, h2d, d2h = [], 0.0, 0.0
+        for _ in range(args.e2e_steps):
+            cc = casgemm.CasCsr()
+            cc.on_device, cc.col_bytes = 0, 4
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            tw = time.perf_counter()
+            stt = ctx.lib.cas_spgemm(ctx.h, casgemm.ACCUM[args.accum], ctypes.byref(ca), ctypes.byref(cb),
+                                     ctypes.byref(cc), None)
+            if stt != 0:
+                raise casgemm.CasError(stt, ctx.lib.cas_last_error(ctx.h).decode())
+            _ = int(np.ctypeslib.as_array(ctypes.cast(cc.row_ptrs, ctypes.POINTER(ctypes.c_int64)), (cc.num_row + 1,))[-1])
+            walls.append(time.perf_counter() - tw)
+            s = ctx.stats()
+            h2d, d2h = s["h2d_bytes"], s["d2h_bytes"]
+            ctx.lib.cas_csr_free(ctx.h, ctypes.byref(cc))
+        wall = statistics.mean(walls)
+        if dist:
+            t = torch.tensor([wall], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        line["e2e"] = {"value": round(2.0 * P_total / wall / 1e9, 3), "unit": "GFLOP/s",
+                       "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                       "steps": args.e2e_steps, "s_per_step": round(wall, 3),
+                       "path": "cas_spgemm on pinned host A, B; C returned in host memory"}
+        del hA, hB
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        dA = dB = None
+        torch.cuda.empty_cache()
+        try:
+            line["cpu_baseline"] = cpu_reference(A, B, args.ref_products, steps=1, warmup=1)
+        except Exception as e:  # reported, not fatal
+            line["cpu_baseline"] = {"value": None, "error": str(e)}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

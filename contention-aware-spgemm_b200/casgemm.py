@@ -26,8 +26,9 @@ STATUS = {
     0: "CAS_OK", 1: "CAS_ERR_BAD_INPUT", 2: "CAS_ERR_OOM", 3: "CAS_ERR_CUDA",
     4: "CAS_ERR_DEVICE", 5: "CAS_ERR_TIMEOUT", 6: "CAS_ERR_ABORTED", 7: "CAS_ERR_REJECTED",
 }
-SYMB_BINS = ["zero", "tiny", "h512", "h2k", "h8k", "h32k", "dense"]
-NUMC_BINS = ["zero", "tiny", "esc1k", "esc2k", "esc4k", "esc8k", "hash256", "hash1k", "hash4k", "dense"]
+SYMB_BINS = ["zero", "tiny", "h1k", "h2k", "h4k", "h8k", "h16k", "h32k", "dense"]
+NUMC_BINS = ["zero", "tiny", "esc1k", "esc2k", "esc3k", "esc4k", "esc5k", "esc6k", "esc8k", "hash256", "hash1k",
+             "hash4k", "dense"]
 
 
 class CasCsr(ctypes.Structure):
@@ -49,8 +50,11 @@ class CasRuntime(ctypes.Structure):
 class CasStats(ctypes.Structure):
     _fields_ = [
         ("flop", ctypes.c_int64), ("max_row_flp", ctypes.c_int64), ("nnz_c", ctypes.c_int64),
-        ("symb_bin_rows", ctypes.c_int64 * 7), ("numc_bin_rows", ctypes.c_int64 * 10),
+        ("symb_bin_rows", ctypes.c_int64 * 9), ("numc_bin_rows", ctypes.c_int64 * 13),
         ("kernel_launches", ctypes.c_int64), ("h2d_bytes", ctypes.c_double), ("d2h_bytes", ctypes.c_double),
+        ("symb_bin_ms", ctypes.c_double * 9), ("numc_bin_ms", ctypes.c_double * 13),
+        ("numc_bin_bytes", ctypes.c_double * 13), ("numc_bin_flop", ctypes.c_int64 * 13),
+        ("esc_overflow_rows", ctypes.c_int64), ("esc_overflow_ms", ctypes.c_double),
     ]
 
 
@@ -78,6 +82,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "cas_set_stream": (I32, [P, P]),
         "cas_set_acc_thres": (I32, [P, D]),
         "cas_last_error": (ctypes.c_char_p, [P]),
+        "cas_set_profiling": (I32, [P, ctypes.c_int]),
         "cas_get_stats": (I32, [P, ctypes.POINTER(CasStats)]),
         "cas_spgemm": (I32, [P, I32, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr),
                              ctypes.POINTER(CasRuntime)]),
@@ -195,6 +200,9 @@ class Context:
     def set_acc_thres(self, thres: float):
         self._check(self.lib.cas_set_acc_thres(self.h, float(thres)))
 
+    def set_profiling(self, on: bool):
+        self._check(self.lib.cas_set_profiling(self.h, int(bool(on))))
+
     def set_stream(self, stream_ptr: Optional[int]):
         self._check(self.lib.cas_set_stream(self.h, stream_ptr))
 
@@ -206,6 +214,11 @@ class Context:
             "symb_bins": dict(zip(SYMB_BINS, list(s.symb_bin_rows))),
             "numc_bins": dict(zip(NUMC_BINS, list(s.numc_bin_rows))),
             "kernel_launches": s.kernel_launches, "h2d_bytes": s.h2d_bytes, "d2h_bytes": s.d2h_bytes,
+            "symb_bin_ms": dict(zip(SYMB_BINS, list(s.symb_bin_ms))),
+            "numc_bin_ms": dict(zip(NUMC_BINS, list(s.numc_bin_ms))),
+            "numc_bin_bytes": dict(zip(NUMC_BINS, list(s.numc_bin_bytes))),
+            "numc_bin_flop": dict(zip(NUMC_BINS, list(s.numc_bin_flop))),
+            "esc_overflow_rows": s.esc_overflow_rows, "esc_overflow_ms": s.esc_overflow_ms,
         }
 
     def spgemm(self, A, B, accum: str = "hybacc", col_bytes: int = 4) -> Result:

@@ -26,15 +26,18 @@
 namespace {
 
 constexpr int kAux = 4;          // auxiliary streams for concurrent bins
-constexpr int kCountSlots = 64;  // device/pinned counter block
+constexpr int kCountSlots = 128; // device/pinned counter block
 
 // Layout of the counter block (unsigned long long slots).
-constexpr int kSlotSymb = 0;     // [0, 7)   symbolic bin counts
-constexpr int kSlotNumc = 8;     // [8, 18)  numeric bin counts
-constexpr int kSlotTotals = 20;  // [20]    products, [21] max row products
-constexpr int kSlotCursor = 24;  // [24, 40) bin cursors
+constexpr int kSlotSymb = 0;     // [0, 9)   symbolic bin counts
+constexpr int kSlotNumc = 10;    // [10, 23) numeric bin counts
+constexpr int kSlotTotals = 24;  // [24]    products, [25] max row products
+constexpr int kSlotCursor = 28;  // [28, 41) bin cursors
 constexpr int kSlotNnz = 44;     // [44]    nnz(C) from the scan
-constexpr int kSlotCheck = 48;   // [48]    input check flags
+constexpr int kSlotCheck = 48;   // [48, 52) input check flags
+constexpr int kSlotBinSums = 64; // [64, 103) per numeric bin: products, nnz(C), nnz(A)
+constexpr int kSlotOvf = 110;    // [110]   rows handed to the radix-sort ESC kernel
+constexpr size_t kStageBytes = size_t(64) << 20;  // pinned staging chunk for host copies
 
 }  // namespace
 
@@ -47,6 +50,10 @@ struct cas_ctx {
   cudaEvent_t ev_fork = nullptr;
   cudaEvent_t ev_join[kAux] = {};
   cudaEvent_t ev_phase[5] = {};
+  cudaEvent_t ev_symb[2][cas::kSymbBins] = {};
+  cudaEvent_t ev_numc[2][cas::kNumcBins] = {};
+  cudaEvent_t ev_ovf[2] = {};
+  bool profile = false;
   double acc_thres = 2.0;
   std::string err;
   cas_stats stats{};
@@ -55,6 +62,8 @@ struct cas_ctx {
   unsigned long long* d_counts = nullptr;
   unsigned long long* h_counts = nullptr;  // pinned mirror
   cas::DevStatus* h_status = nullptr;      // pinned mirror
+  void* h_stage[2] = {};                   // pinned staging for large host copies
+  cudaEvent_t ev_stage[2] = {};
 };
 
 namespace {
@@ -89,7 +98,9 @@ cas_status set_err(cas_ctx* ctx, cas_status st, const char* fmt, ...) {
 cas_status check_launch(cas_ctx* ctx, const char* what) {
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return set_err(ctx, CAS_ERR_CUDA, "launch of %s failed: %s", what, cudaGetErrorString(e));
+  if (e != cudaSuccess)
+    return set_err(ctx, CAS_ERR_CUDA, "launch of %s failed: %s (stream %p)", what, cudaGetErrorString(e),
+                   (void*)ctx->stream);
   return CAS_OK;
 }
 
@@ -122,8 +133,8 @@ cas_status allow_smem(cas_ctx* ctx, K kernel, size_t bytes) {
 }
 
 // ------------------------------------------------ kernel shapes and memory
-template <int BLOCK, int TBITS>
-constexpr size_t smem_symb_hash() { return (size_t(1) << TBITS) * 4 + sizeof(cas::Stage<double>); }
+template <int BLOCK, int TBITS, int SEGCAP>
+constexpr size_t smem_symb_hash() { return (size_t(1) << TBITS) * 4 + SEGCAP + sizeof(cas::StageB<double>); }
 template <int BLOCK>
 constexpr size_t smem_symb_dense() { return size_t(cas::kDenseChunkBits / 32) * 4 + sizeof(cas::Stage<double>); }
 template <int BLOCK, int CAP, typename VIn>
@@ -142,13 +153,42 @@ constexpr size_t smem_numc_dense() {
          sizeof(cas::Stage<VIn>);
 }
 
+template <int CAP, int NBB, typename VIn>
+constexpr size_t smem_numc_esc_msd() {
+  return size_t(CAP) * (sizeof(typename cas::Acc<VIn>::T) + 4) + (size_t(1) << NBB) * 2 +
+         (size_t(1) << NBB) / 32 * 4 + ((size_t(CAP) * 2 + 15) & ~size_t(15)) + sizeof(cas::StageB<VIn>);
+}
+
+// symbolic hash shape of each symbolic bin: threads, log2(table slots), byte
+// table capacity (shared memory allows 3 CTAs per SM for the 16 Ki table)
+#define CAS_SYMB_SHAPES(X)        \
+  X(kSB_H1K, 128, 10, 1024)       \
+  X(kSB_H2K, 128, 11, 2048)       \
+  X(kSB_H4K, 256, 12, 4096)       \
+  X(kSB_H8K, 256, 13, 4096)       \
+  X(kSB_H16K, 256, 14, 8192)      \
+  X(kSB_H32K, 512, 15, 16384)
+
+// bucketed ESC shape of each ESC bin: capacity and log2(bucket count), two to
+// four products per bucket; shared memory allows 8, 6, 4, 3, 3, 2, 1 CTAs of
+// 256 threads per SM for the seven bins
+#define CAS_ESC_SHAPES(X) \
+  X(kNB_E1K, 1024, 9)   \
+  X(kNB_E2K, 2048, 9)   \
+  X(kNB_E3K, 3072, 10)  \
+  X(kNB_E4K, 4096, 10)  \
+  X(kNB_E5K, 4800, 11)  \
+  X(kNB_E6K, 6144, 11)  \
+  X(kNB_E8K, 8192, 11)
+
 template <typename VIn>
 cas_status setup_numc_kernels(cas_ctx* ctx) {
   using namespace cas;
-  CAS_TRY(allow_smem(ctx, k_numc_esc<256, 1024, VIn>, smem_numc_esc<256, 1024, VIn>()));
-  CAS_TRY(allow_smem(ctx, k_numc_esc<256, 2048, VIn>, smem_numc_esc<256, 2048, VIn>()));
-  CAS_TRY(allow_smem(ctx, k_numc_esc<512, 4096, VIn>, smem_numc_esc<512, 4096, VIn>()));
-  CAS_TRY(allow_smem(ctx, k_numc_esc<1024, 8192, VIn>, smem_numc_esc<1024, 8192, VIn>()));
+#define CAS_SETUP_ESC(bin, CAP, NBB) \
+  CAS_TRY(allow_smem(ctx, k_numc_esc_msd<256, CAP, NBB, VIn>, smem_numc_esc_msd<CAP, NBB, VIn>()));
+  CAS_ESC_SHAPES(CAS_SETUP_ESC)
+#undef CAS_SETUP_ESC
+  CAS_TRY(allow_smem(ctx, k_numc_esc_overflow<1024, 8192, VIn>, smem_numc_esc<1024, 8192, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_hash<256, 9, VIn>, smem_numc_hash<256, 9, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_hash<256, 11, VIn>, smem_numc_hash<256, 11, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_hash<512, 13, VIn>, smem_numc_hash<512, 13, VIn>()));
@@ -158,10 +198,9 @@ cas_status setup_numc_kernels(cas_ctx* ctx) {
 
 cas_status setup_kernels(cas_ctx* ctx) {
   using namespace cas;
-  CAS_TRY(allow_smem(ctx, k_symb_hash<128, 9>, smem_symb_hash<128, 9>()));
-  CAS_TRY(allow_smem(ctx, k_symb_hash<256, 11>, smem_symb_hash<256, 11>()));
-  CAS_TRY(allow_smem(ctx, k_symb_hash<512, 13>, smem_symb_hash<512, 13>()));
-  CAS_TRY(allow_smem(ctx, k_symb_hash<1024, 15>, smem_symb_hash<1024, 15>()));
+#define CAS_SETUP_SYMB(bin, BLK, TB, SEG) CAS_TRY(allow_smem(ctx, k_symb_hash<BLK, TB, SEG>, smem_symb_hash<BLK, TB, SEG>()));
+  CAS_SYMB_SHAPES(CAS_SETUP_SYMB)
+#undef CAS_SETUP_SYMB
   CAS_TRY(allow_smem(ctx, k_symb_dense<1024>, smem_symb_dense<1024>()));
   CAS_TRY(setup_numc_kernels<double>(ctx));
   CAS_TRY(setup_numc_kernels<int32_t>(ctx));
@@ -196,6 +235,41 @@ cas_status dev_alloc(cas_ctx* ctx, void** p, size_t bytes) {
     cudaGetLastError();
     return set_err(ctx, e == cudaErrorMemoryAllocation ? CAS_ERR_OOM : CAS_ERR_CUDA,
                    "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+  }
+  return CAS_OK;
+}
+
+// Device -> pageable host copy through two pinned staging buffers: the copy
+// of chunk i runs on the DMA engine while host threads move chunk i-1 out of
+// staging (and fault in the destination pages in parallel).
+cas_status d2h_staged(cas_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return CAS_OK;
+  if (!ctx->h_stage[0]) {
+    for (int i = 0; i < 2; ++i) {
+      CAS_CUDA(ctx, cudaMallocHost(&ctx->h_stage[i], kStageBytes));
+      CAS_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_stage[i], cudaEventDisableTiming));
+    }
+  }
+  const size_t nchunk = (bytes + kStageBytes - 1) / kStageBytes;
+  for (size_t i = 0; i <= nchunk; ++i) {
+    if (i < nchunk) {
+      const size_t off = i * kStageBytes, len = std::min(kStageBytes, bytes - off);
+      CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage[i & 1], static_cast<const char*>(src) + off, len,
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+      CAS_CUDA(ctx, cudaEventRecord(ctx->ev_stage[i & 1], ctx->stream));
+    }
+    if (i > 0) {
+      const size_t j = i - 1, off = j * kStageBytes, len = std::min(kStageBytes, bytes - off);
+      CAS_CUDA(ctx, cudaEventSynchronize(ctx->ev_stage[j & 1]));
+      char* d = static_cast<char*>(dst) + off;
+      const char* s = static_cast<const char*>(ctx->h_stage[j & 1]);
+      const int64_t pieces = (int64_t)((len + (1 << 20) - 1) >> 20);
+#pragma omp parallel for schedule(static)
+      for (int64_t p = 0; p < pieces; ++p) {
+        const size_t o = (size_t)p << 20;
+        memcpy(d + o, s + o, std::min((size_t)1 << 20, len - o));
+      }
+    }
   }
   return CAS_OK;
 }
@@ -294,9 +368,11 @@ struct Call {
   int64_t* row_flp = nullptr;
   int64_t* row_nz = nullptr;
   int32_t* rows = nullptr;
+  int32_t* ovf = nullptr;  // rows the bucketed ESC kernel hands to the radix-sort ESC kernel
   int64_t* partial = nullptr;
   int64_t nparts = 0;
   bool b_sorted = true;
+  bool ovf_launched = false;
   int64_t symb_count[cas::kSymbBins] = {};
   int64_t numc_count[cas::kNumcBins] = {};
   int64_t flop = 0, max_flp = 0;
@@ -319,17 +395,18 @@ cas_status scratch_alloc(cas_ctx* ctx, Call& c) {
   CAS_TRY(dev_alloc(ctx, (void**)&c.row_flp, sizeof(int64_t) * (c.m + 1)));
   CAS_TRY(dev_alloc(ctx, (void**)&c.row_nz, sizeof(int64_t) * (c.m + 1)));
   CAS_TRY(dev_alloc(ctx, (void**)&c.rows, sizeof(int32_t) * (c.m + 1)));
+  CAS_TRY(dev_alloc(ctx, (void**)&c.ovf, sizeof(int32_t) * (c.m + 1)));
   c.nparts = (c.m + 1 + cas::kScanTile - 1) / cas::kScanTile;
   CAS_TRY(dev_alloc(ctx, (void**)&c.partial, sizeof(int64_t) * (c.nparts + 1)));
   return CAS_OK;
 }
 
 cas_status scratch_free(cas_ctx* ctx, Call& c) {
-  void* ps[] = {c.row_flp, c.row_nz, c.rows, c.partial};
+  void* ps[] = {c.row_flp, c.row_nz, c.rows, c.ovf, c.partial};
   for (void* p : ps)
     if (p) CAS_CUDA(ctx, cudaFreeAsync(p, ctx->stream));
   c.row_flp = c.row_nz = nullptr;
-  c.rows = nullptr;
+  c.rows = c.ovf = nullptr;
   c.partial = nullptr;
   return CAS_OK;
 }
@@ -407,29 +484,25 @@ cas_status launch_symb_bins(cas_ctx* ctx, Call& c, int64_t* row_nz) {
   int64_t off[kSymbBins + 1] = {0};
   for (int b = 0; b < kSymbBins; ++b) off[b + 1] = off[b] + c.symb_count[b];
   // heaviest bins first, each on its own stream
-  const int order[] = {kSB_Dense, kSB_H32K, kSB_H8K, kSB_H2K, kSB_H512, kSB_Tiny};
+  const int order[] = {kSB_Dense, kSB_H32K, kSB_H16K, kSB_H8K, kSB_H4K, kSB_H2K, kSB_H1K, kSB_Tiny};
   int si = 0;
   for (int b : order) {
     const int64_t n = c.symb_count[b];
     if (n == 0) continue;
     const int32_t* rows = c.rows + off[b];
-    cudaStream_t s = ctx->aux[si++ % kAux];
+    cudaStream_t s = ctx->profile ? ctx->stream : ctx->aux[si++ % kAux];  // profiling: one bin at a time
+    if (ctx->profile) CAS_CUDA(ctx, cudaEventRecord(ctx->ev_symb[0][b], s));
     switch (b) {
       case kSB_Tiny:
         k_symb_tiny<256><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(rows, n, c.A.csr, c.B.csr, row_nz, ctx->d_status);
         break;
-      case kSB_H512:
-        k_symb_hash<128, 9><<<(unsigned)n, 128, smem_symb_hash<128, 9>(), s>>>(rows, c.A.csr, c.B.csr, row_nz, ctx->d_status);
+#define CAS_SYMB_CASE(bin, BLK, TB, SEG)                                                              \
+      case bin:                                                                                     \
+        k_symb_hash<BLK, TB, SEG><<<(unsigned)n, BLK, smem_symb_hash<BLK, TB, SEG>(), s>>>(          \
+            rows, c.A.csr, c.B.csr, row_nz, ctx->d_status);                                         \
         break;
-      case kSB_H2K:
-        k_symb_hash<256, 11><<<(unsigned)n, 256, smem_symb_hash<256, 11>(), s>>>(rows, c.A.csr, c.B.csr, row_nz, ctx->d_status);
-        break;
-      case kSB_H8K:
-        k_symb_hash<512, 13><<<(unsigned)n, 512, smem_symb_hash<512, 13>(), s>>>(rows, c.A.csr, c.B.csr, row_nz, ctx->d_status);
-        break;
-      case kSB_H32K:
-        k_symb_hash<1024, 15><<<(unsigned)n, 1024, smem_symb_hash<1024, 15>(), s>>>(rows, c.A.csr, c.B.csr, row_nz, ctx->d_status);
-        break;
+      CAS_SYMB_SHAPES(CAS_SYMB_CASE)
+#undef CAS_SYMB_CASE
       case kSB_Dense:
         if (!c.b_sorted && c.ncol > kDenseChunkBits)
           return set_err(ctx, CAS_ERR_BAD_INPUT, "heavy rows over more than %d columns need B rows sorted by column", kDenseChunkBits);
@@ -437,6 +510,7 @@ cas_status launch_symb_bins(cas_ctx* ctx, Call& c, int64_t* row_nz) {
         break;
     }
     CAS_TRY(check_launch(ctx, "symbolic bin"));
+    if (ctx->profile) CAS_CUDA(ctx, cudaEventRecord(ctx->ev_symb[1][b], s));
   }
   CAS_TRY(join(ctx));
   return CAS_OK;
@@ -446,13 +520,18 @@ cas_status launch_symb_bins(cas_ctx* ctx, Call& c, int64_t* row_nz) {
 cas_status numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int mode) {
   using namespace cas;
   CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + kSlotNumc, 0, sizeof(unsigned long long) * kNumcBins, ctx->stream));
+  CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + kSlotBinSums, 0, sizeof(unsigned long long) * 3 * kNumcBins,
+                                ctx->stream));
   if (c.m > 0) {
     k_bin_count_numc<<<grid_for(c.m, 256, ctx->sm_count * 8), 256, 0, ctx->stream>>>(
-        c.m, c.row_flp, crp, mode, ctx->acc_thres, ctx->d_counts + kSlotNumc);
+        c.m, c.row_flp, crp, c.A.csr.rp, mode, ctx->acc_thres, ctx->d_counts + kSlotNumc,
+        ctx->d_counts + kSlotBinSums);
     CAS_TRY(check_launch(ctx, "k_bin_count_numc"));
   }
   CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotNumc, ctx->d_counts + kSlotNumc,
                                 sizeof(unsigned long long) * kNumcBins, cudaMemcpyDeviceToHost, ctx->stream));
+  CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotBinSums, ctx->d_counts + kSlotBinSums,
+                                sizeof(unsigned long long) * 3 * kNumcBins, cudaMemcpyDeviceToHost, ctx->stream));
   CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   unsigned long long* cur = ctx->h_counts + kSlotCursor;
   unsigned long long off = 0;
@@ -477,34 +556,35 @@ cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* 
   using namespace cas;
   using AT = typename Acc<VIn>::T;
   AT* cval = static_cast<AT*>(cval_v);
-  CAS_TRY(fork(ctx));
   int64_t off[kNumcBins + 1] = {0};
   for (int b = 0; b < kNumcBins; ++b) off[b + 1] = off[b] + c.numc_count[b];
-  const int order[] = {kNB_Dense, kNB_E8K, kNB_H4K, kNB_E4K, kNB_H1K, kNB_E2K, kNB_E1K, kNB_H256, kNB_Tiny};
+  const int order[] = {kNB_Dense, kNB_E8K, kNB_H4K, kNB_E6K, kNB_E5K, kNB_E4K, kNB_E3K, kNB_H1K,
+                       kNB_E2K, kNB_E1K, kNB_H256, kNB_Tiny};
+  unsigned int* ovf_count = reinterpret_cast<unsigned int*>(ctx->d_counts + kSlotOvf);
+  CAS_CUDA(ctx, cudaMemsetAsync(ovf_count, 0, sizeof(unsigned int), ctx->stream));
+  CAS_TRY(fork(ctx));
+  int64_t esc_rows = 0;
   int si = 0;
   for (int b : order) {
     const int64_t n = c.numc_count[b];
     if (n == 0) continue;
     const int32_t* rows = c.rows + off[b];
-    cudaStream_t s = ctx->aux[si++ % kAux];
+    cudaStream_t s = ctx->profile ? ctx->stream : ctx->aux[si++ % kAux];  // profiling: one bin at a time
+    if (ctx->profile) CAS_CUDA(ctx, cudaEventRecord(ctx->ev_numc[0][b], s));
     const Csr& A = c.A.csr;
     const Csr& B = c.B.csr;
     switch (b) {
       case kNB_Tiny:
         k_numc_tiny<256, VIn><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(rows, n, A, B, crp, ccol, cval, ctx->d_status);
         break;
-      case kNB_E1K:
-        k_numc_esc<256, 1024, VIn><<<(unsigned)n, 256, smem_numc_esc<256, 1024, VIn>(), s>>>(rows, A, B, crp, ccol, cval, ctx->d_status);
+#define CAS_ESC_CASE(bin, CAP, NBB)                                                                     \
+      case bin:                                                                                         \
+        esc_rows += n;                                                                                  \
+        k_numc_esc_msd<256, CAP, NBB, VIn><<<(unsigned)n, 256, smem_numc_esc_msd<CAP, NBB, VIn>(), s>>>( \
+            rows, A, B, c.b_sorted ? 1 : 0, crp, ccol, cval, c.ovf, ovf_count, ctx->d_status);          \
         break;
-      case kNB_E2K:
-        k_numc_esc<256, 2048, VIn><<<(unsigned)n, 256, smem_numc_esc<256, 2048, VIn>(), s>>>(rows, A, B, crp, ccol, cval, ctx->d_status);
-        break;
-      case kNB_E4K:
-        k_numc_esc<512, 4096, VIn><<<(unsigned)n, 512, smem_numc_esc<512, 4096, VIn>(), s>>>(rows, A, B, crp, ccol, cval, ctx->d_status);
-        break;
-      case kNB_E8K:
-        k_numc_esc<1024, 8192, VIn><<<(unsigned)n, 1024, smem_numc_esc<1024, 8192, VIn>(), s>>>(rows, A, B, crp, ccol, cval, ctx->d_status);
-        break;
+      CAS_ESC_SHAPES(CAS_ESC_CASE)
+#undef CAS_ESC_CASE
       case kNB_H256:
         k_numc_hash<256, 9, VIn><<<(unsigned)n, 256, smem_numc_hash<256, 9, VIn>(), s>>>(rows, A, B, crp, ccol, cval, ctx->d_status);
         break;
@@ -521,8 +601,19 @@ cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* 
         break;
     }
     CAS_TRY(check_launch(ctx, "numeric bin"));
+    if (ctx->profile) CAS_CUDA(ctx, cudaEventRecord(ctx->ev_numc[1][b], s));
   }
   CAS_TRY(join(ctx));
+  if (esc_rows > 0) {
+    // rows whose columns bucket unevenly: radix-sort ESC, one persistent CTA per SM
+    if (ctx->profile) CAS_CUDA(ctx, cudaEventRecord(ctx->ev_ovf[0], ctx->stream));
+    k_numc_esc_overflow<1024, 8192, VIn><<<(unsigned)std::min<int64_t>(esc_rows, ctx->sm_count), 1024,
+                                          smem_numc_esc<1024, 8192, VIn>(), ctx->stream>>>(
+        c.ovf, ovf_count, c.A.csr, c.B.csr, crp, ccol, cval, ctx->d_status);
+    CAS_TRY(check_launch(ctx, "k_numc_esc_overflow"));
+    if (ctx->profile) CAS_CUDA(ctx, cudaEventRecord(ctx->ev_ovf[1], ctx->stream));
+    c.ovf_launched = true;
+  }
   return CAS_OK;
 }
 
@@ -531,6 +622,9 @@ int mode_of(cas_accum a) {
 }
 
 cas_status prepare(cas_ctx* ctx, const cas_csr* A, const cas_csr* B, Call& c, double& h2d) {
+  // launches are checked with cudaGetLastError, which also returns an error
+  // another library in the process left behind; start from a clean slate
+  cudaGetLastError();
   CAS_TRY(basic_checks(ctx, A, "A"));
   CAS_TRY(basic_checks(ctx, B, "B"));
   if (A->num_col != B->num_row)
@@ -582,6 +676,8 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
   else CAS_TRY(launch_numc_bins<int32_t>(ctx, c, crp, ccol, cval));
   CAS_TRY(scratch_free(ctx, c));
   CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[4], ctx->stream));
+  CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotOvf, ctx->d_counts + kSlotOvf, sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, ctx->stream));
   CAS_TRY(check_status(ctx));
   CAS_TRY(free_owned(ctx, c.A));
   CAS_TRY(free_owned(ctx, c.B));
@@ -608,17 +704,17 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
       memset(C, 0, sizeof(*C));
       return set_err(ctx, CAS_ERR_OOM, "host allocation of C failed");
     }
-    CAS_CUDA(ctx, cudaMemcpyAsync(C->row_ptrs, crp, sizeof(int64_t) * (c.m + 1), cudaMemcpyDeviceToHost, ctx->stream));
-    CAS_CUDA(ctx, cudaMemcpyAsync(C->rats, cval, vbytes * nnz, cudaMemcpyDeviceToHost, ctx->stream));
+    CAS_TRY(d2h_staged(ctx, C->row_ptrs, crp, sizeof(int64_t) * (c.m + 1)));
+    CAS_TRY(d2h_staged(ctx, C->rats, cval, vbytes * nnz));
     if (c_col_bytes == 4) {
-      CAS_CUDA(ctx, cudaMemcpyAsync(C->cols, ccol, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, ctx->stream));
-      CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      CAS_TRY(d2h_staged(ctx, C->cols, ccol, sizeof(int32_t) * nnz));
     } else {
-      std::vector<int32_t> tmp((size_t)nnz);
-      CAS_CUDA(ctx, cudaMemcpyAsync(tmp.data(), ccol, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, ctx->stream));
-      CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      // widen into the upper half-free int64 buffer: copy int32 into its
+      // first half, then widen from the back so nothing is overwritten early
+      CAS_TRY(d2h_staged(ctx, C->cols, ccol, sizeof(int32_t) * nnz));
+      const int32_t* c32 = static_cast<const int32_t*>(C->cols);
       int64_t* c64 = static_cast<int64_t*>(C->cols);
-      for (int64_t i = 0; i < nnz; ++i) c64[i] = tmp[(size_t)i];
+      for (int64_t i = nnz - 1; i >= 0; --i) c64[i] = c32[i];
     }
     d2h += sizeof(int64_t) * (double)(c.m + 1) + (vbytes + c_col_bytes) * (double)nnz;
     CAS_CUDA(ctx, cudaFreeAsync(crp, ctx->stream));
@@ -644,6 +740,33 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
   s.kernel_launches = ctx->launches;
   s.h2d_bytes = h2d;
   s.d2h_bytes = d2h;
+  const double vin = c.vt == CAS_VAL_F64 ? 8.0 : 4.0;
+  for (int b = 0; b < kNumcBins; ++b) {
+    const double flp = (double)ctx->h_counts[kSlotBinSums + b];
+    const double nzc = (double)ctx->h_counts[kSlotBinSums + kNumcBins + b];
+    const double nza = (double)ctx->h_counts[kSlotBinSums + 2 * kNumcBins + b];
+    s.numc_bin_flop[b] = (int64_t)ctx->h_counts[kSlotBinSums + b];
+    s.numc_bin_bytes[b] = (4 + vin) * (nza + flp) + 12.0 * nzc + 16.0 * (double)c.numc_count[b];
+    s.numc_bin_ms[b] = 0;
+    float ms = 0;
+    if (ctx->profile && c.numc_count[b] > 0 &&
+        cudaEventElapsedTime(&ms, ctx->ev_numc[0][b], ctx->ev_numc[1][b]) == cudaSuccess)
+      s.numc_bin_ms[b] = ms;
+  }
+  s.esc_overflow_rows = (int64_t)(ctx->h_counts[kSlotOvf] & 0xFFFFFFFFull);
+  s.esc_overflow_ms = 0;
+  {
+    float ms = 0;
+    if (ctx->profile && c.ovf_launched && cudaEventElapsedTime(&ms, ctx->ev_ovf[0], ctx->ev_ovf[1]) == cudaSuccess)
+      s.esc_overflow_ms = ms;
+  }
+  for (int b = 0; b < kSymbBins; ++b) {
+    s.symb_bin_ms[b] = 0;
+    float ms = 0;
+    if (ctx->profile && c.symb_count[b] > 0 &&
+        cudaEventElapsedTime(&ms, ctx->ev_symb[0][b], ctx->ev_symb[1][b]) == cudaSuccess)
+      s.symb_bin_ms[b] = ms;
+  }
   return CAS_OK;
 }
 
@@ -669,6 +792,11 @@ cas_status cas_create(int device, cas_ctx** out) {
     }
     CAS_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
     for (int i = 0; i < 5; ++i) CAS_CUDA(ctx, cudaEventCreate(&ctx->ev_phase[i]));
+    for (int i = 0; i < 2; ++i) {
+      CAS_CUDA(ctx, cudaEventCreate(&ctx->ev_ovf[i]));
+      for (int b = 0; b < cas::kSymbBins; ++b) CAS_CUDA(ctx, cudaEventCreate(&ctx->ev_symb[i][b]));
+      for (int b = 0; b < cas::kNumcBins; ++b) CAS_CUDA(ctx, cudaEventCreate(&ctx->ev_numc[i][b]));
+    }
     CAS_CUDA(ctx, cudaMalloc(&ctx->d_status, sizeof(cas::DevStatus)));
     CAS_CUDA(ctx, cudaMalloc(&ctx->d_counts, sizeof(unsigned long long) * kCountSlots));
     CAS_CUDA(ctx, cudaMallocHost(&ctx->h_counts, sizeof(unsigned long long) * kCountSlots));
@@ -701,10 +829,21 @@ void cas_destroy(cas_ctx* ctx) {
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   for (int i = 0; i < 5; ++i)
     if (ctx->ev_phase[i]) cudaEventDestroy(ctx->ev_phase[i]);
+  for (int i = 0; i < 2; ++i) {
+    if (ctx->ev_ovf[i]) cudaEventDestroy(ctx->ev_ovf[i]);
+    for (int b = 0; b < cas::kSymbBins; ++b)
+      if (ctx->ev_symb[i][b]) cudaEventDestroy(ctx->ev_symb[i][b]);
+    for (int b = 0; b < cas::kNumcBins; ++b)
+      if (ctx->ev_numc[i][b]) cudaEventDestroy(ctx->ev_numc[i][b]);
+  }
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->d_counts) cudaFree(ctx->d_counts);
   if (ctx->h_counts) cudaFreeHost(ctx->h_counts);
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
+  for (int i = 0; i < 2; ++i) {
+    if (ctx->h_stage[i]) cudaFreeHost(ctx->h_stage[i]);
+    if (ctx->ev_stage[i]) cudaEventDestroy(ctx->ev_stage[i]);
+  }
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
 }
@@ -722,6 +861,12 @@ cas_status cas_set_acc_thres(cas_ctx* ctx, double thres) {
 }
 
 const char* cas_last_error(const cas_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+cas_status cas_set_profiling(cas_ctx* ctx, int on) {
+  if (!ctx) return CAS_ERR_BAD_INPUT;
+  ctx->profile = on != 0;
+  return CAS_OK;
+}
 
 cas_status cas_get_stats(const cas_ctx* ctx, cas_stats* out) {
   if (!ctx || !out) return CAS_ERR_BAD_INPUT;

@@ -63,17 +63,26 @@ __global__ void k_bin_scatter_symb(int64_t m, const int64_t* __restrict__ row_fl
   }
 }
 
+// Numeric bin histogram plus, per bin, the sums of products, nnz(C) and
+// nnz(A) of its rows (for the per-kernel algorithmic byte count).
 __global__ void k_bin_count_numc(int64_t m, const int64_t* __restrict__ row_flp, const int64_t* __restrict__ crp,
-                                 int mode, double thres, unsigned long long* __restrict__ bin_count) {
-  __shared__ unsigned long long s_cnt[kNumcBins];
-  if (threadIdx.x < kNumcBins) s_cnt[threadIdx.x] = 0;
+                                 const int64_t* __restrict__ arp, int mode, double thres,
+                                 unsigned long long* __restrict__ bin_count, unsigned long long* __restrict__ bin_sums) {
+  __shared__ unsigned long long s_cnt[4 * kNumcBins];
+  if (threadIdx.x < 4 * kNumcBins) s_cnt[threadIdx.x] = 0;
   __syncthreads();
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
-    const int b = numc_bin_of(row_flp[r], crp[r + 1] - crp[r], mode, thres);
+    const int64_t flp = row_flp[r], nz = crp[r + 1] - crp[r];
+    const int b = numc_bin_of(flp, nz, mode, thres);
     atomicAdd(&s_cnt[b], 1ull);
+    atomicAdd(&s_cnt[kNumcBins + b], (unsigned long long)flp);
+    atomicAdd(&s_cnt[2 * kNumcBins + b], (unsigned long long)nz);
+    atomicAdd(&s_cnt[3 * kNumcBins + b], (unsigned long long)(arp[r + 1] - arp[r]));
   }
   __syncthreads();
   if (threadIdx.x < kNumcBins && s_cnt[threadIdx.x]) atomicAdd(&bin_count[threadIdx.x], s_cnt[threadIdx.x]);
+  if (threadIdx.x >= kNumcBins && threadIdx.x < 4 * kNumcBins && s_cnt[threadIdx.x])
+    atomicAdd(&bin_sums[threadIdx.x - kNumcBins], s_cnt[threadIdx.x]);
 }
 
 __global__ void k_bin_scatter_numc(int64_t m, const int64_t* __restrict__ row_flp, const int64_t* __restrict__ crp,
@@ -156,7 +165,7 @@ k_scan_apply(const int64_t* __restrict__ in, int64_t n_in, const int64_t* __rest
 // `ranged`, every B row is cut to the columns [c0, c1) by binary search (B
 // rows sorted); otherwise f receives every product.
 constexpr int kAChunk = 256;
-constexpr int kUnroll = 4;
+constexpr int kUnroll = 8;
 
 template <typename VIn>
 struct alignas(16) Stage {
@@ -191,7 +200,12 @@ __device__ __forceinline__ int64_t expand_row(const Csr& A, const Csr& B, int64_
     long long total;
     const long long ex = block_exclusive_sum<BLOCK, long long>(len, sg.tmp, total);
     if (threadIdx.x < ACH) sg.pre[threadIdx.x] = ex;
+    if (threadIdx.x == 0) sg.pre[na] = total;
     __syncthreads();
+    // A entry of product p: the interpolated guess p * na / total, checked
+    // with its neighbours (exact for rows of near-equal B row lengths), else
+    // a binary search for the last entry whose prefix is <= p.
+    const float per = total > 0 ? (float)na / (float)total : 0.f;
     for (int64_t p0 = threadIdx.x; p0 < total; p0 += (int64_t)BLOCK * kUnroll) {
       int32_t key[kUnroll];
       VIn bv[kUnroll];
@@ -201,11 +215,31 @@ __device__ __forceinline__ int64_t expand_row(const Csr& A, const Csr& B, int64_
         const int64_t p = p0 + (int64_t)u * BLOCK;
         sgi[u] = -1;
         if (p < total) {
-          int lo = 0, hi = na;
-          while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (sg.pre[mid] <= p) lo = mid; else hi = mid;
+          int s = min(na - 1, (int)((float)p * per));
+          if (sg.pre[s] > p) {
+            if (s > 0 && sg.pre[s - 1] <= p) {
+              --s;
+            } else {
+              int lo = 0, hi = s;
+              while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (sg.pre[mid] <= p) lo = mid; else hi = mid;
+              }
+              s = lo;
+            }
+          } else if (sg.pre[s + 1] <= p) {
+            if (sg.pre[s + 2] > p) {
+              ++s;
+            } else {
+              int lo = s + 2, hi = na;
+              while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (sg.pre[mid] <= p) lo = mid; else hi = mid;
+              }
+              s = lo;
+            }
           }
+          const int lo = s;
           const int64_t j = sg.bs[lo] + (p - sg.pre[lo]);
           key[u] = __ldg(B.col + j);
           if (NEED_VAL) bv[u] = __ldg(bval + j);
@@ -278,41 +312,6 @@ k_symb_tiny(const int32_t* __restrict__ rows, int64_t nrows, Csr A, Csr B, int64
   const bool lead = (mykey >> 32) == 0 && lane == __ffs(peers) - 1;
   const int cnt = __popc(__ballot_sync(kFull, lead));
   if (lane == 0) row_nz[r] = cnt;
-}
-
-// Rows whose distinct columns fit a shared-memory hash of 2^TBITS keys (at
-// least twice the bound min(row_flp, num_col)): linear probing on 32-bit keys,
-// one atomicCAS per new key; the count is the number of successful inserts
-// (ams_hash_symb_krnl, src/ams/ams_utils.c:101-164, in shared memory).
-template <int BLOCK, int TBITS>
-__global__ void __launch_bounds__(BLOCK)
-k_symb_hash(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t* __restrict__ row_nz, DevStatus* st) {
-  constexpr int T = 1 << TBITS;
-  extern __shared__ __align__(16) uint8_t smem[];
-  uint32_t* tab = reinterpret_cast<uint32_t*>(smem);
-  Stage<double>& sg = *reinterpret_cast<Stage<double>*>(smem + T * sizeof(uint32_t));
-  const int64_t r = rows[blockIdx.x];
-  for (int i = threadIdx.x; i < T; i += BLOCK) tab[i] = kEmptyKey;
-  __syncthreads();
-  long long cnt = 0;
-  bool full = false;
-  expand_row<BLOCK, false, double>(A, B, r, sg, false, 0, 0, [&](int32_t key, double, double, int64_t) {
-    uint32_t h = hash_slot((uint32_t)key, TBITS);
-    for (int probe = 0; probe < T; ++probe) {
-      const uint32_t cur = tab[h];
-      if (cur == (uint32_t)key) return;
-      if (cur == kEmptyKey) {
-        const uint32_t old = atomicCAS(&tab[h], kEmptyKey, (uint32_t)key);
-        if (old == kEmptyKey) { ++cnt; return; }
-        if (old == (uint32_t)key) return;
-      }
-      h = (h + 1) & (T - 1);
-    }
-    full = true;
-  });
-  if (full) dev_report(st, kDevTableFull, 2, r);
-  cnt = block_sum<BLOCK, long long>(cnt, sg.tmp);
-  if (threadIdx.x == 0) row_nz[r] = cnt;
 }
 
 // Heavy rows: a bitmap over kDenseChunkBits columns at a time; the count is
@@ -450,11 +449,10 @@ struct alignas(16) SortScratch {
 // equal columns (ams_hsersc_numc_krnl, src/ams/ams_utils.c:399-456).  The
 // sort is stable, so each sum is taken in expansion order.
 template <int BLOCK, int CAP, typename VIn>
-__global__ void __launch_bounds__(BLOCK)
-k_numc_esc(const int32_t* __restrict__ rows, Csr A, Csr B, const int64_t* __restrict__ crp,
-           int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval, DevStatus* st) {
+__device__ __forceinline__ void esc_radix_row(int64_t r, const Csr& A, const Csr& B, const int64_t* __restrict__ crp,
+                                              int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval,
+                                              DevStatus* st, uint8_t* smem) {
   using AT = typename Acc<VIn>::T;
-  extern __shared__ __align__(16) uint8_t smem[];
   uint64_t* items = reinterpret_cast<uint64_t*>(smem);
   uint64_t* items2 = items + CAP;
   AT* ev = reinterpret_cast<AT*>(items2 + CAP);
@@ -462,7 +460,6 @@ k_numc_esc(const int32_t* __restrict__ rows, Csr A, Csr B, const int64_t* __rest
   Stage<VIn>& sg = *reinterpret_cast<Stage<VIn>*>(reinterpret_cast<uint8_t*>(&ss) + sizeof(SortScratch<BLOCK>));
   __shared__ uint32_t s_min, s_max;
   __shared__ int s_over;
-  const int64_t r = rows[blockIdx.x];
   if (threadIdx.x == 0) { s_min = 0xFFFFFFFFu; s_max = 0u; s_over = 0; }
   __syncthreads();
   uint32_t kmin = 0xFFFFFFFFu, kmax = 0u;
@@ -513,6 +510,421 @@ k_numc_esc(const int32_t* __restrict__ rows, Csr A, Csr B, const int64_t* __rest
     carry += tot;
   }
   if (threadIdx.x == 0 && carry != nz) dev_report(st, carry > nz ? kDevRowOverflow : kDevRowUnderflow, 11, r);
+}
+
+template <int BLOCK, int CAP, typename VIn>
+__global__ void __launch_bounds__(BLOCK)
+k_numc_esc(const int32_t* __restrict__ rows, Csr A, Csr B, const int64_t* __restrict__ crp,
+           int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval, DevStatus* st) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  esc_radix_row<BLOCK, CAP, VIn>(rows[blockIdx.x], A, B, crp, ccol, cval, st, smem);
+}
+
+// Persistent form for the rows the bucketed ESC kernel hands back (their
+// keys fall unevenly into its buckets): the list length is read on the device.
+template <int BLOCK, int CAP, typename VIn>
+__global__ void __launch_bounds__(BLOCK)
+k_numc_esc_overflow(const int32_t* __restrict__ rows, const unsigned int* __restrict__ count, Csr A, Csr B,
+                    const int64_t* __restrict__ crp, int32_t* __restrict__ ccol,
+                    typename Acc<VIn>::T* __restrict__ cval, DevStatus* st) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const unsigned n = *count;
+  for (unsigned i = blockIdx.x; i < n; i += gridDim.x) {
+    esc_radix_row<BLOCK, CAP, VIn>(rows[i], A, B, crp, ccol, cval, st, smem);
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row expansion for the capacity-bounded kernels (a row's products fit in
+// shared memory).  A entries are staged kBChunk at a time; each chunk's
+// product-to-entry map is a byte table written once per B row with coalesced
+// stores, so finding a product's A entry is one shared-memory byte load, and
+// all product indices are 32-bit.  When B's rows are sorted, the row's column
+// range [kmin, kmax] is known from each B row's first and last column before
+// any product is read.
+constexpr int kBChunk = 128;  // A entries per staged chunk (uniform R-MAT rows have ~64)
+
+template <typename VIn>
+struct alignas(16) StageB {
+  int64_t bs[kBChunk];       // start of the B row (global index)
+  int32_t pre[kBChunk + 1];  // exclusive prefix of B row lengths in the chunk
+  VIn av[kBChunk];
+  int tmp[34];
+  uint32_t kmin, kmax;
+  int over;
+};
+
+// Stages one chunk of A entries [a0, a0+na) and fills segof; returns the
+// chunk's product count.  With `range`, also reduces the first/last columns
+// of the B rows into sg.kmin / sg.kmax (B rows sorted by column).
+template <int BLOCK, bool NEED_VAL, typename VIn>
+__device__ __forceinline__ int stage_chunk(const Csr& A, const Csr& B, int64_t a0, int na, StageB<VIn>& sg,
+                                           uint8_t* __restrict__ segof, int cap, bool range) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = BLOCK / 32;
+  int len = 0;
+  uint32_t lo_key = 0xFFFFFFFFu, hi_key = 0u;
+  if (threadIdx.x < na) {
+    const int32_t k = A.col[a0 + threadIdx.x];
+    const int64_t lo = B.rp[k], hi = B.rp[k + 1];
+    sg.bs[threadIdx.x] = lo;
+    len = (int)(hi - lo);
+    if (NEED_VAL) sg.av[threadIdx.x] = static_cast<const VIn*>(A.val)[a0 + threadIdx.x];
+    if (range && hi > lo) {
+      lo_key = (uint32_t)__ldg(B.col + lo);
+      hi_key = (uint32_t)__ldg(B.col + hi - 1);
+    }
+  }
+  if (range) {
+    lo_key = warp_min_u32(lo_key);
+    hi_key = warp_max_u32(hi_key);
+    if (lane == 0 && hi_key >= lo_key) {
+      atomicMin(&sg.kmin, lo_key);
+      atomicMax(&sg.kmax, hi_key);
+    }
+  }
+  int total;
+  const int ex = block_exclusive_sum<BLOCK, int>(len, sg.tmp, total);
+  if (threadIdx.x < na) sg.pre[threadIdx.x] = ex;
+  if (threadIdx.x == 0) sg.pre[na] = total;
+  __syncthreads();
+  if (total <= cap) {
+    for (int sgi = warp; sgi < na; sgi += NW) {
+      const int b0 = sg.pre[sgi], l = sg.pre[sgi + 1] - b0;
+      for (int i = lane; i < l; i += 32) segof[b0 + i] = (uint8_t)sgi;
+    }
+  }
+  __syncthreads();
+  return total;
+}
+
+// Product p (< total) of the staged chunk: calls f(key, a, b, p).  Loads of
+// kUnroll products are issued before any is consumed.
+template <int BLOCK, bool NEED_VAL, typename VIn, typename F>
+__device__ __forceinline__ void expand_chunk(const Csr& B, int total, const StageB<VIn>& sg,
+                                             const uint8_t* __restrict__ segof, F&& f) {
+  const VIn* __restrict__ bval = static_cast<const VIn*>(B.val);
+  for (int p0 = threadIdx.x; p0 < total; p0 += BLOCK * kUnroll) {
+    int32_t key[kUnroll];
+    VIn bv[kUnroll];
+    int sgi[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int p = p0 + u * BLOCK;
+      sgi[u] = -1;
+      if (p < total) {
+        const int s = segof[p];
+        const int64_t j = sg.bs[s] + (p - sg.pre[s]);
+        key[u] = __ldg(B.col + j);
+        if (NEED_VAL) bv[u] = __ldg(bval + j);
+        sgi[u] = s;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      if (sgi[u] >= 0) f(key[u], NEED_VAL ? sg.av[sgi[u]] : VIn(0), NEED_VAL ? bv[u] : VIn(0), p0 + u * BLOCK);
+    }
+  }
+}
+
+// Two 16-bit bucket counters per 32-bit word (shared-memory atomics are
+// 32-bit); counts and offsets stay below 2^16 because CAP <= 32768.
+__device__ __forceinline__ uint32_t bucket_add(uint32_t* w, int b) {
+  const uint32_t sh = (b & 1) << 4;
+  return (atomicAdd(&w[b >> 1], 1u << sh) >> sh) & 0xFFFFu;
+}
+__device__ __forceinline__ uint32_t bucket_get(const uint32_t* w, int b) { return (w[b >> 1] >> ((b & 1) << 4)) & 0xFFFFu; }
+
+__device__ __forceinline__ void cswap(uint32_t& ka, uint32_t& pa, uint32_t& kb, uint32_t& pb) {
+  const bool sw = kb < ka;
+  const uint32_t k0 = sw ? kb : ka, k1 = sw ? ka : kb, p0 = sw ? pb : pa, p1 = sw ? pa : pb;
+  ka = k0; kb = k1; pa = p0; pb = p1;
+}
+
+// Batcher's odd-even merge sort network for 8 inputs (19 comparators).
+__device__ __forceinline__ void sort8(uint32_t (&k)[8], uint32_t (&p)[8]) {
+  cswap(k[0], p[0], k[1], p[1]); cswap(k[2], p[2], k[3], p[3]);
+  cswap(k[4], p[4], k[5], p[5]); cswap(k[6], p[6], k[7], p[7]);
+  cswap(k[0], p[0], k[2], p[2]); cswap(k[1], p[1], k[3], p[3]);
+  cswap(k[4], p[4], k[6], p[6]); cswap(k[5], p[5], k[7], p[7]);
+  cswap(k[1], p[1], k[2], p[2]); cswap(k[5], p[5], k[6], p[6]);
+  cswap(k[0], p[0], k[4], p[4]); cswap(k[1], p[1], k[5], p[5]);
+  cswap(k[2], p[2], k[6], p[6]); cswap(k[3], p[3], k[7], p[7]);
+  cswap(k[2], p[2], k[4], p[4]); cswap(k[3], p[3], k[5], p[5]);
+  cswap(k[1], p[1], k[2], p[2]); cswap(k[3], p[3], k[4], p[4]);
+  cswap(k[5], p[5], k[6], p[6]);
+}
+
+// Products of a staged chunk too large for the byte table: the A entry of
+// product p is found by binary search over the 32-bit prefixes.
+template <int BLOCK, typename VIn, typename F>
+__device__ __forceinline__ void expand_chunk_search(const Csr& B, int na, int total, const StageB<VIn>& sg, F&& f) {
+  for (int p0 = threadIdx.x; p0 < total; p0 += BLOCK * kUnroll) {
+    int32_t key[kUnroll];
+    bool ok[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int p = p0 + u * BLOCK;
+      ok[u] = p < total;
+      if (ok[u]) {
+        int lo = 0, hi = na;
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (sg.pre[mid] <= p) lo = mid; else hi = mid;
+        }
+        key[u] = __ldg(B.col + sg.bs[lo] + (p - sg.pre[lo]));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u)
+      if (ok[u]) f(key[u]);
+  }
+}
+
+// Symbolic phase for rows whose distinct columns fit a shared-memory hash of
+// 2^TBITS keys (at least twice the bound min(row_flp, num_col)): linear
+// probing on 32-bit keys, claiming a slot with atomicCAS directly (most
+// products bring a new column in the rows this serves); the count is the
+// number of successful claims (ams_hash_symb_krnl, src/ams/ams_utils.c:101-164,
+// in shared memory).  A chunk of at most SEGCAP products uses the byte table
+// to map products to A entries, a larger one binary search.
+template <int BLOCK, int TBITS, int SEGCAP>
+__global__ void __launch_bounds__(BLOCK)
+k_symb_hash(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t* __restrict__ row_nz, DevStatus* st) {
+  constexpr int T = 1 << TBITS;
+  constexpr int ACH = BLOCK < kBChunk ? BLOCK : kBChunk;
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint32_t* tab = reinterpret_cast<uint32_t*>(smem);
+  uint8_t* segof = reinterpret_cast<uint8_t*>(tab + T);
+  StageB<double>& sg = *reinterpret_cast<StageB<double>*>(segof + SEGCAP);
+  const int64_t r = rows[blockIdx.x];
+  const int64_t as = A.rp[r], ae = A.rp[r + 1];
+  for (int i = threadIdx.x; i < T / 4; i += BLOCK) reinterpret_cast<uint4*>(tab)[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
+  __syncthreads();
+  int cnt = 0;
+  bool full = false;
+  auto insert = [&](int32_t key) {
+    uint32_t h = hash_slot((uint32_t)key, TBITS);
+    for (int probe = 0; probe < T; ++probe) {
+      const uint32_t old = atomicCAS(&tab[h], kEmptyKey, (uint32_t)key);
+      if (old == kEmptyKey) { ++cnt; return; }
+      if (old == (uint32_t)key) return;
+      h = (h + 1) & (T - 1);
+    }
+    full = true;
+  };
+  for (int64_t a0 = as; a0 < ae; a0 += ACH) {
+    const int na = (int)((ae - a0) < (int64_t)ACH ? (ae - a0) : (int64_t)ACH);
+    const int total = stage_chunk<BLOCK, false, double>(A, B, a0, na, sg, segof, SEGCAP, false);
+    if (total <= SEGCAP)
+      expand_chunk<BLOCK, false, double>(B, total, sg, segof, [&](int32_t key, double, double, int) { insert(key); });
+    else
+      expand_chunk_search<BLOCK, double>(B, na, total, sg, insert);
+    __syncthreads();
+  }
+  if (full) dev_report(st, kDevTableFull, 2, r);
+  int tot;
+  block_exclusive_sum<BLOCK, int>(cnt, sg.tmp, tot);
+  if (threadIdx.x == 0) row_nz[r] = tot;
+}
+
+// ESC accumulator with a one-pass bucket sort, for rows of at most CAP
+// products (ams_hsersc_numc_krnl, src/ams/ams_utils.c:399-456): expand
+// (column, a*b) into shared memory while histogramming the products into
+// NB = 2^NBB buckets (about four products per bucket) by the high bits of
+// (column - min column); scatter product indices into bucket order; sort each
+// bucket — one lane per bucket, an 8-input sorting network for the usual
+// buckets of at most 8 products, insertion sort beyond; then sum runs of equal
+// columns, 32 sorted entries per warp step so a warp's stores are contiguous.
+// A row with a bucket of more than kBucketLimit products (columns crowded into
+// a narrow range) is appended to `ovf` and left to the radix-sort ESC kernel.
+// The limit counts products, not distinct columns: the diagonal column of
+// A*A^T alone puts |A_i| products into one bucket, and equal keys cost the
+// insertion sort little.  Shared memory: 14 bytes per product plus half a
+// byte per bucket.
+constexpr int kBucketLimit = 96;
+
+template <int BLOCK, int CAP, int NBB, typename VIn>
+__global__ void __launch_bounds__(BLOCK)
+k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted, const int64_t* __restrict__ crp,
+               int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval,
+               int32_t* __restrict__ ovf, unsigned int* __restrict__ ovf_count, DevStatus* st) {
+  using AT = typename Acc<VIn>::T;
+  constexpr int NB = 1 << NBB;
+  constexpr int NW = BLOCK / 32;
+  constexpr int NG = NB / 32;
+  constexpr int ACH = BLOCK < kBChunk ? BLOCK : kBChunk;
+  static_assert(kBChunk <= 256, "8-bit A entry indices");
+  static_assert(CAP <= 32768 && CAP % 32 == 0, "16-bit indices and counters");
+  static_assert(NG <= BLOCK && NB % (2 * BLOCK) == 0, "one group count per thread; whole counter words per thread");
+  extern __shared__ __align__(16) uint8_t smem[];
+  AT* sval = reinterpret_cast<AT*>(smem);
+  uint32_t* skey = reinterpret_cast<uint32_t*>(sval + CAP);
+  uint32_t* bcnt = skey + CAP;                 // NB 16-bit counters
+  uint32_t* gcnt = bcnt + NB / 2;              // NG group counts / offsets
+  uint16_t* perm = reinterpret_cast<uint16_t*>(gcnt + NG);
+  uint8_t* segof = reinterpret_cast<uint8_t*>(perm);  // used only while expanding, before perm is written
+  StageB<VIn>& sg = *reinterpret_cast<StageB<VIn>*>(reinterpret_cast<uint8_t*>(perm) + ((CAP * 2 + 15) & ~15));
+  const int64_t r = rows[blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t as = A.rp[r], ae = A.rp[r + 1];
+  if (threadIdx.x == 0) { sg.kmin = 0xFFFFFFFFu; sg.kmax = 0u; sg.over = 0; }
+  for (int i = threadIdx.x; i < NB / 2; i += BLOCK) bcnt[i] = 0u;
+  // the column range first: from the staged chunk when the row has one chunk,
+  // else from a pass over all its A entries (or [0, num_col) when B is unsorted)
+  const bool one_chunk = ae - as <= ACH;
+  if (!one_chunk) {
+    __syncthreads();
+    if (b_sorted) {
+      uint32_t lo_key = 0xFFFFFFFFu, hi_key = 0u;
+      for (int64_t ja = as + threadIdx.x; ja < ae; ja += BLOCK) {
+        const int32_t k = A.col[ja];
+        const int64_t lo = B.rp[k], hi = B.rp[k + 1];
+        if (hi > lo) {
+          lo_key = min(lo_key, (uint32_t)__ldg(B.col + lo));
+          hi_key = max(hi_key, (uint32_t)__ldg(B.col + hi - 1));
+        }
+      }
+      lo_key = warp_min_u32(lo_key);
+      hi_key = warp_max_u32(hi_key);
+      if (lane == 0) {
+        atomicMin(&sg.kmin, lo_key);
+        atomicMax(&sg.kmax, hi_key);
+      }
+    } else if (threadIdx.x == 0) {
+      sg.kmin = 0u;
+      sg.kmax = (uint32_t)(B.ncol > 0 ? B.ncol - 1 : 0);
+    }
+  } else if (!b_sorted && threadIdx.x == 0) {
+    sg.kmin = 0u;
+    sg.kmax = (uint32_t)(B.ncol > 0 ? B.ncol - 1 : 0);
+  }
+  __syncthreads();
+  int n = 0;
+  for (int64_t a0 = as; a0 < ae; a0 += ACH) {
+    const int na = (int)((ae - a0) < (int64_t)ACH ? (ae - a0) : (int64_t)ACH);
+    const int total = stage_chunk<BLOCK, true, VIn>(A, B, a0, na, sg, segof, CAP - n, one_chunk && b_sorted);
+    if (n + total > CAP) {  // uniform: the bin bound was violated
+      if (threadIdx.x == 0) dev_report(st, kDevCapacity, 14, r);
+      return;
+    }
+    const uint32_t lo = sg.kmin, range = sg.kmax - sg.kmin;
+    const int bits = (sg.kmax > sg.kmin) ? 32 - __clz(range) : 0;
+    const int shift = bits > NBB ? bits - NBB : 0;
+    const int base = n;
+    expand_chunk<BLOCK, true, VIn>(B, total, sg, segof, [&](int32_t key, VIn av, VIn bv, int p) {
+      skey[base + p] = (uint32_t)key;
+      sval[base + p] = Acc<VIn>::mul(av, bv);
+      bucket_add(bcnt, (int)(((uint32_t)key - lo) >> shift));
+    });
+    n += total;
+    __syncthreads();
+  }
+  const uint32_t lo = sg.kmin, range = sg.kmax - sg.kmin;
+  const int bits = (sg.kmax > sg.kmin) ? 32 - __clz(range) : 0;
+  const int shift = bits > NBB ? bits - NBB : 0;
+  // exclusive scan of the bucket counts: NB / BLOCK consecutive buckets per thread
+  constexpr int WPT = NB / (2 * BLOCK);
+  uint32_t loc[WPT];
+  uint32_t sum = 0, big = 0;
+#pragma unroll
+  for (int i = 0; i < WPT; ++i) {
+    loc[i] = bcnt[threadIdx.x * WPT + i];
+    const uint32_t c0 = loc[i] & 0xFFFFu, c1 = loc[i] >> 16;
+    sum += c0 + c1;
+    big = max(big, max(c0, c1));
+  }
+  if (__syncthreads_or(big > (uint32_t)kBucketLimit)) {
+    if (threadIdx.x == 0) ovf[atomicAdd(ovf_count, 1u)] = (int32_t)r;
+    return;
+  }
+  int tot_all;
+  uint32_t run = (uint32_t)block_exclusive_sum<BLOCK, int>((int)sum, sg.tmp, tot_all);
+#pragma unroll
+  for (int i = 0; i < WPT; ++i) {
+    const uint32_t c0 = loc[i] & 0xFFFFu, c1 = loc[i] >> 16;
+    bcnt[threadIdx.x * WPT + i] = run | ((run + c0) << 16);
+    run += c0 + c1;
+  }
+  __syncthreads();
+  // scatter product indices into bucket order; bucket b then ends at bucket_get(b)
+  for (int p = threadIdx.x; p < n; p += BLOCK) perm[bucket_add(bcnt, (int)((skey[p] - lo) >> shift))] = (uint16_t)p;
+  __syncthreads();
+  // one lane per bucket: sort it by column, count its distinct columns
+  for (int g = warp; g < NG; g += NW) {
+    const int b = g * 32 + lane;
+    const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
+    const int nb = e - s;
+    int heads;
+    if (nb <= 8) {
+      uint32_t k[8], q[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        q[i] = i < nb ? perm[s + i] : 0u;
+        k[i] = i < nb ? skey[q[i]] : 0xFFFFFFFFu;
+      }
+      sort8(k, q);
+      heads = nb > 0;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        if (i < nb) perm[s + i] = (uint16_t)q[i];
+        if (i > 0 && i < nb) heads += k[i] != k[i - 1];
+      }
+    } else {
+      for (int i = s + 1; i < e; ++i) {
+        const uint16_t pi = perm[i];
+        const uint32_t ki = skey[pi];
+        int j = i - 1;
+        while (j >= s && skey[perm[j]] > ki) {
+          perm[j + 1] = perm[j];
+          --j;
+        }
+        perm[j + 1] = pi;
+      }
+      heads = 1;
+      for (int i = s + 1; i < e; ++i) heads += skey[perm[i]] != skey[perm[i - 1]];
+    }
+    heads = warp_sum(heads);
+    if (lane == 0) gcnt[g] = (uint32_t)heads;
+  }
+  __syncthreads();
+  int total;
+  {
+    const int c = threadIdx.x < NG ? (int)gcnt[threadIdx.x] : 0;
+    const int ex = block_exclusive_sum<BLOCK, int>(c, sg.tmp, total);
+    if (threadIdx.x < NG) gcnt[threadIdx.x] = (uint32_t)ex;
+  }
+  __syncthreads();
+  // each group's sorted entries, 32 at a time: run heads write (column, sum)
+  // to consecutive positions.  Equal columns share a bucket, so no run
+  // crosses a group.
+  const int64_t c0 = crp[r], nz = crp[r + 1] - c0;
+  for (int g = warp; g < NG; g += NW) {
+    const int gs = g ? (int)bucket_get(bcnt, g * 32 - 1) : 0, ge = (int)bucket_get(bcnt, g * 32 + 31);
+    int64_t out = gcnt[g];
+    for (int e0 = gs; e0 < ge; e0 += 32) {
+      const int t = e0 + lane;
+      bool head = false;
+      uint32_t key = 0;
+      if (t < ge) {
+        key = skey[perm[t]];
+        head = t == gs || key != skey[perm[t - 1]];
+      }
+      const unsigned hm = __ballot_sync(kFull, head);
+      if (head) {
+        AT v = sval[perm[t]];
+        for (int t2 = t + 1; t2 < ge && skey[perm[t2]] == key; ++t2) v += sval[perm[t2]];
+        const int64_t pos = out + __popc(hm & lanemask_lt());
+        if (pos < nz) {
+          ccol[c0 + pos] = (int32_t)key;
+          cval[c0 + pos] = v;
+        }
+      }
+      out += __popc(hm);
+    }
+  }
+  if (threadIdx.x == 0 && total != nz) dev_report(st, total > nz ? kDevRowOverflow : kDevRowUnderflow, 14, r);
 }
 
 // Hash accumulator for rows with at most 2^TBITS / 2 distinct columns: linear

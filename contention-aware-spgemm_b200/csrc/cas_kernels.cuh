@@ -25,29 +25,37 @@ namespace cas {
 // ------------------------------------------------------------ parameters
 // Symbolic bins by t = min(row_flp, num_col) (an upper bound on the row's
 // distinct columns); numeric bins by accumulator and size.
+// Hash tables hold at least twice the bound, so the load factor stays <= 1/2.
 enum SymbBin : int {
   kSB_Zero = 0,    // row_flp == 0
   kSB_Tiny = 1,    // row_flp <= 32: one warp, one product per lane
-  kSB_H512 = 2,    // t <= 256:   128 threads, 512-slot table
-  kSB_H2K = 3,     // t <= 1024:  256 threads, 2048-slot table
-  kSB_H8K = 4,     // t <= 4096:  512 threads, 8192-slot table
-  kSB_H32K = 5,    // t <= 16384: 1024 threads, 32768-slot table
-  kSB_Dense = 6,   // larger: column bitmap in shared memory
-  kSymbBins = 7
+  kSB_H1K = 2,     // t <= 512:   128 threads, 1024-slot table
+  kSB_H2K = 3,     // t <= 1024:  128 threads, 2048-slot table
+  kSB_H4K = 4,     // t <= 2048:  256 threads, 4096-slot table
+  kSB_H8K = 5,     // t <= 4096:  256 threads, 8192-slot table (32 KiB)
+  kSB_H16K = 6,    // t <= 8192:  256 threads, 16384-slot table (64 KiB)
+  kSB_H32K = 7,    // t <= 16384: 512 threads, 32768-slot table (128 KiB)
+  kSB_Dense = 8,   // larger: column bitmap in shared memory
+  kSymbBins = 9
 };
 
+// ESC bins by products (bucketed ESC, 256 threads; capacity = the bound);
+// hash bins by nnz of the row.
 enum NumcBin : int {
   kNB_Zero = 0,    // no products
   kNB_Tiny = 1,    // row_flp <= 32: warp sort in registers
-  kNB_E1K = 2,     // ESC, row_flp <= 1024 (256 threads)
-  kNB_E2K = 3,     // ESC, row_flp <= 2048 (256 threads)
-  kNB_E4K = 4,     // ESC, row_flp <= 4096 (512 threads)
-  kNB_E8K = 5,     // ESC, row_flp <= 8192 (1024 threads)
-  kNB_H256 = 6,    // hash, nnz <= 256   (128 threads, 512 slots)
-  kNB_H1K = 7,     // hash, nnz <= 1024  (256 threads, 2048 slots)
-  kNB_H4K = 8,     // hash, nnz <= 4096  (512 threads, 8192 slots)
-  kNB_Dense = 9,   // dense column chunks in shared memory
-  kNumcBins = 10
+  kNB_E1K = 2,     // ESC, row_flp <= 1024
+  kNB_E2K = 3,     // ESC, row_flp <= 2048
+  kNB_E3K = 4,     // ESC, row_flp <= 3072
+  kNB_E4K = 5,     // ESC, row_flp <= 4096
+  kNB_E5K = 6,     // ESC, row_flp <= 4800
+  kNB_E6K = 7,     // ESC, row_flp <= 6144
+  kNB_E8K = 8,     // ESC, row_flp <= 8192
+  kNB_H256 = 9,    // hash, nnz <= 256   (256 threads, 512 slots)
+  kNB_H1K = 10,    // hash, nnz <= 1024  (256 threads, 2048 slots)
+  kNB_H4K = 11,    // hash, nnz <= 4096  (512 threads, 8192 slots)
+  kNB_Dense = 12,  // dense column chunks in shared memory
+  kNumcBins = 13
 };
 
 enum AccumMode : int { kAccHash = 0, kAccEsc = 1, kAccHybrid = 2 };
@@ -66,9 +74,11 @@ __host__ __device__ __forceinline__ int symb_bin_of(int64_t flp, int64_t ncol) {
   if (flp <= 0) return kSB_Zero;
   if (flp <= 32) return kSB_Tiny;
   const int64_t t = flp < ncol ? flp : ncol;
-  if (t <= 256) return kSB_H512;
+  if (t <= 512) return kSB_H1K;
   if (t <= 1024) return kSB_H2K;
+  if (t <= 2048) return kSB_H4K;
   if (t <= 4096) return kSB_H8K;
+  if (t <= 8192) return kSB_H16K;
   if (t <= 16384) return kSB_H32K;
   return kSB_Dense;
 }
@@ -83,7 +93,10 @@ __host__ __device__ __forceinline__ int numc_bin_of(int64_t flp, int64_t nz, int
   if (esc) {
     if (flp <= 1024) return kNB_E1K;
     if (flp <= 2048) return kNB_E2K;
+    if (flp <= 3072) return kNB_E3K;
     if (flp <= 4096) return kNB_E4K;
+    if (flp <= 4800) return kNB_E5K;
+    if (flp <= 6144) return kNB_E6K;
     if (flp <= 8192) return kNB_E8K;
   }
   if (nz <= 256) return kNB_H256;

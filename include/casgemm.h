@@ -73,8 +73,8 @@ typedef struct {
 	double total_time;
 } cas_runtime;
 
-#define CAS_SYMB_BINS 7
-#define CAS_NUMC_BINS 10
+#define CAS_SYMB_BINS 9
+#define CAS_NUMC_BINS 13
 
 /* Counters of the last cas_spgemm call. */
 typedef struct {
@@ -86,6 +86,18 @@ typedef struct {
 	int64_t kernel_launches;               /* kernels launched by the library since cas_create */
 	double h2d_bytes;                      /* host->device bytes copied by the call */
 	double d2h_bytes;                      /* device->host bytes copied by the call */
+	/* with cas_set_profiling(ctx, 1): device time of each bin's kernel (ms,
+	 * CUDA events on the stream it ran on) and, for the numeric bins, the
+	 * algorithmic bytes of its rows: 12*nnz(A rows) + 12*products +
+	 * 12*nnz(C rows) + 16*rows for fp64 (int32 in / int64 out: 8/8/12/16). */
+	double symb_bin_ms[CAS_SYMB_BINS];
+	double numc_bin_ms[CAS_NUMC_BINS];
+	double numc_bin_bytes[CAS_NUMC_BINS];
+	int64_t numc_bin_flop[CAS_NUMC_BINS];
+	/* rows the bucketed ESC kernel handed to the radix-sort ESC kernel (their
+	 * columns crowd into a narrow range), and that kernel's time (profiling) */
+	int64_t esc_overflow_rows;
+	double esc_overflow_ms;
 } cas_stats;
 
 typedef struct cas_ctx cas_ctx;
@@ -100,6 +112,10 @@ cas_status cas_set_stream(cas_ctx *ctx, void *stream);
  * script's value for ams_hybaccspgemm (scripts/ams_rmat_run.sh:33). */
 cas_status cas_set_acc_thres(cas_ctx *ctx, double thres);
 const char *cas_last_error(const cas_ctx *ctx);
+/* 1: run the bins one after another on the context's stream and time every
+ * bin kernel with CUDA events (cas_stats.*_bin_ms); 0 (default): bins run
+ * concurrently on auxiliary streams. */
+cas_status cas_set_profiling(cas_ctx *ctx, int on);
 cas_status cas_get_stats(const cas_ctx *ctx, cas_stats *out);
 
 /* ---- the reference's phase functions, on device CSR (col_bytes 4) ------ */

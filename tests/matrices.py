@@ -30,7 +30,7 @@ def cases():
     for s, ef in [(6, 2), (8, 4), (10, 8), (12, 8), (12, 16)]:
         A = casgemm.gen_g500(s, ef, 100 + s)
         out.append((f"g500_s{s}_ef{ef}", A, A.transpose()))
-    for s, ef in [(10, 4), (12, 32)]:
+    for s, ef in [(10, 4), (12, 32), (13, 32)]:
         A = casgemm.gen_er(s, ef, 200 + s)
         out.append((f"er_s{s}_ef{ef}", A, A.transpose()))
     Z = casgemm.gen_zipf(4000, 20000, 800, 40000, 7, col_q=50.0)
