@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -986,3 +987,57 @@ cas_status cas_hybacc_numc(cas_ctx* ctx, const cas_csr* A, const cas_csr* B, con
 }
 
 }  // extern "C"
+
+// ===================================================== scan without allocation
+// cas_scan_noalloc: the same exclusive scan as cas_scan, for callers that must
+// not allocate device memory — for example a process whose device memory is
+// handed out by another framework's pool and budget, where a cudaMalloc behind
+// its back breaks the accounting, or a latency-sensitive loop that cannot take
+// the device-wide synchronisation a cudaMalloc or cudaFree may imply.  The
+// per-tile partial sums live in a fixed array in device memory, created when
+// the library is loaded and kept by every device that loads it until the
+// process exits (kNoAllocParts partials, 128 KiB).  Every call overwrites the
+// partials it reads before reading them, so nothing needs clearing, and calls
+// that overlap on the GPU (on different streams, or from several host threads)
+// share the array and race: serialise them.
+namespace {
+
+constexpr int64_t kNoAllocParts = 16384;  // scans of up to kNoAllocParts * kScanTile elements
+constexpr int kNoAllocMaxDevices = 256;
+
+static __device__ __align__(256) int64_t g_noalloc_partials[kNoAllocParts];
+
+std::mutex g_noalloc_mu;
+int64_t* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+}  // namespace
+
+extern "C" cas_status cas_scan_noalloc(int64_t* d_out, const int64_t* d_in, int64_t n, void* stream) {
+  if (!d_out || n < 0 || (n > 1 && !d_in)) return CAS_ERR_BAD_INPUT;
+  if (n == 0) return CAS_OK;
+  const int64_t nparts = (n + cas::kScanTile - 1) / cas::kScanTile;
+  if (nparts > kNoAllocParts) return CAS_ERR_REJECTED;  // n > kNoAllocParts * kScanTile
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return CAS_ERR_CUDA;
+  int64_t* partial = nullptr;
+  {
+    // first call on this device: look up the array's device address (the
+    // host-side name of a __device__ variable is not a device pointer)
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) {
+        cudaGetLastError();
+        return CAS_ERR_CUDA;
+      }
+      g_noalloc_addr[dev] = static_cast<int64_t*>(p);
+    }
+    partial = g_noalloc_addr[dev];
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaGetLastError();  // start from a clean error state, as the context entry points do
+  cas::k_scan_partials<<<(unsigned)nparts, cas::kScanBlock, 0, s>>>(d_in, n - 1, partial);
+  cas::k_scan_top<<<1, cas::kScanBlock, 0, s>>>(partial, nparts, nullptr);
+  cas::k_scan_apply<<<(unsigned)nparts, cas::kScanBlock, 0, s>>>(d_in, n - 1, partial, d_out, n);
+  return cudaGetLastError() == cudaSuccess ? CAS_OK : CAS_ERR_CUDA;
+}

@@ -161,6 +161,28 @@ cas_status cas_spgemm(cas_ctx *ctx, cas_accum accum, const cas_csr *A, const cas
 /* Frees arrays the library allocated (owned != 0) and zeroes the struct. */
 cas_status cas_csr_free(cas_ctx *ctx, cas_csr *C);
 
+/* ---- scan that allocates nothing ---------------------------------------- */
+
+/* The exclusive scan of cas_scan (d_out[0] = 0, d_out[i+1] = d_out[i] +
+ * d_in[i], device arrays of the current device) for callers that must not
+ * allocate device memory: a process whose device memory is owned and
+ * budgeted by another framework's pool, or a latency-sensitive loop that
+ * cannot afford the synchronisation a cudaMalloc/cudaFree may bring.  It
+ * needs no context and calls no allocator: its scratch is a fixed 128 KiB
+ * array in device memory that every device loading the library keeps until
+ * the process exits.
+ *   - n may be at most 67,108,864 (16,384 tiles of 4,096); larger n returns
+ *     CAS_ERR_REJECTED without touching memory.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - The call is asynchronous on `stream` (a cudaStream_t as void*, NULL for
+ *     the default stream); synchronise before reading d_out.
+ *   - All calls share the one array: calls that may overlap on the GPU must
+ *     be serialised by the caller.
+ * No counterpart in the reference: its scan (src/mm/mm_utils.c:903) runs on
+ * the host and allocates nothing on a device to begin with. */
+cas_status cas_scan_noalloc(int64_t *d_out, const int64_t *d_in, int64_t n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
