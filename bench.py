@@ -56,26 +56,19 @@ def make_matrix(name):
 
 
 def row_products(A, B):
-    """Prefix of intermediate products over the rows of A (length num_row + 1)."""
-    cnt = np.diff(B.row_ptrs)[A.cols].astype(np.int64)
-    return np.concatenate([[0], np.cumsum(cnt)])[A.row_ptrs]
+    import casgemm
+    return casgemm.row_products_prefix(A, B)
 
 
 def row_shard(A, B, rank, world, r_end):
-    """Contiguous rows [r0, r1) of [0, r_end) holding about 1/world of their products."""
-    if world == 1:
-        return 0, r_end
-    ps = row_products(A, B)[: r_end + 1]
-    total = int(ps[-1])
-    r0 = int(np.searchsorted(ps, total * rank // world, side="left"))
-    r1 = int(np.searchsorted(ps, total * (rank + 1) // world, side="left")) if rank + 1 < world else r_end
-    return r0, r1
+    import casgemm
+    return casgemm.row_shard(row_products(A, B) if world > 1 else np.zeros(A.num_row + 1, np.int64), rank, world,
+                             r_end)
 
 
 def slice_rows(A, r0, r1):
     import casgemm
-    s, e = int(A.row_ptrs[r0]), int(A.row_ptrs[r1])
-    return casgemm.Csr(r1 - r0, A.num_col, A.row_ptrs[r0:r1 + 1] - s, A.cols[s:e], A.vals[s:e])
+    return casgemm.slice_rows(A, r0, r1)
 
 
 def sample_rows_for(A, B, target_products):

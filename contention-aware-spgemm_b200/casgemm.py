@@ -344,3 +344,33 @@ def mtx_write(path: str, A: Csr, symmetric: bool):
     if load().cas_mtx_write(path.encode(), A.num_row, A.num_col, _ptr(np.ascontiguousarray(A.row_ptrs, np.int64)),
                             _ptr(np.ascontiguousarray(A.cols, np.int32)), int(symmetric)) != 0:
         raise ValueError(f"cannot write {path}")
+
+
+# ---------------------------------------------------------- row sharding
+def row_products_prefix(A: Csr, B: Csr) -> np.ndarray:
+    """Prefix of intermediate products over the rows of A (num_row + 1 entries)."""
+    cnt = np.diff(B.row_ptrs)[np.asarray(A.cols, dtype=np.int64)].astype(np.int64)
+    return np.concatenate([[0], np.cumsum(cnt)])[A.row_ptrs]
+
+
+def row_shard(prefix: np.ndarray, rank: int, world: int, r_end: Optional[int] = None):
+    """Contiguous rows [r0, r1) of [0, r_end) holding about 1/world of their products.
+
+    Rows of C are independent (C[r0:r1] = A[r0:r1] * B), so shards need no
+    exchange; splitting by the product prefix is the lower_bound-on-prefix
+    split of the reference's morsel packing (src/ams/ams_utils.c:1459-1465)."""
+    n = len(prefix) - 1
+    r_end = n if r_end is None else r_end
+    if world <= 1:
+        return 0, r_end
+    ps = prefix[: r_end + 1]
+    total = int(ps[-1])
+    r0 = 0 if rank == 0 else int(np.searchsorted(ps, total * rank // world, side="left"))
+    r1 = r_end if rank + 1 == world else int(np.searchsorted(ps, total * (rank + 1) // world, side="left"))
+    return r0, r1
+
+
+def slice_rows(A: Csr, r0: int, r1: int) -> Csr:
+    """Rows [r0, r1) of A as a CSR of its own (views, no copy of columns/values)."""
+    s, e = int(A.row_ptrs[r0]), int(A.row_ptrs[r1])
+    return Csr(r1 - r0, A.num_col, A.row_ptrs[r0:r1 + 1] - s, A.cols[s:e], A.vals[s:e])

@@ -161,6 +161,19 @@ def ref_spgemm(A, B, algo: str = "hybacc", small: bool = True):
     return rp, cols, vals, {n: getattr(rt, n) for n, _ in RefRuntime._fields_}
 
 
+def ref_load_mtx(path: str):
+    """The reference's own MatrixMarket loader: (num_row, num_col, row_ptrs, cols, vals)."""
+    lib = _load_ref("hybacc", True)
+    lib.ref_load_mtx.argtypes = [ctypes.c_char_p, ctypes.POINTER(OrcCsr)]
+    m = OrcCsr()
+    lib.ref_load_mtx(path.encode(), ctypes.byref(m))
+    try:
+        rp, cols, vals = _from_orc(m)
+        return m.num_row, m.num_col, rp, cols, vals
+    finally:
+        lib.ref_free_csr(ctypes.byref(m))
+
+
 def ref_info(algo: str = "hybacc", small: bool = False) -> dict:
     lib = _load_ref(algo, small)
     return {"threads": lib.ref_thread_num(), "morsel": lib.ref_morsel_size(), "acc_thres": lib.ref_acc_thres()}

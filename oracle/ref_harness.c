@@ -68,6 +68,14 @@ long ref_intprod(csr_t *A, csr_t *B) {
 	return (long) p;
 }
 
+/* The reference's MatrixMarket loader (raw2csr -> mtx2csr -> mtx2trpl ->
+ * trpl2csr, src/mm/mm_utils.c:451-692, 730) into M; release with ref_free_csr. */
+void ref_load_mtx(const char *path, csr_t *M) {
+	ref_setup();
+	memset(M, 0, sizeof(csr_t));
+	raw2csr(M, path, &numa_cfg);
+}
+
 void ref_free_csr(csr_t *C) {
 	if (C->row_ptrs) {
 		free_csr(C);
