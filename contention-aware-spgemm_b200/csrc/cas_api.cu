@@ -156,8 +156,8 @@ constexpr size_t smem_numc_dense() {
 
 template <int CAP, int NBB, typename VIn>
 constexpr size_t smem_numc_esc_msd() {
-  return size_t(CAP) * (sizeof(typename cas::Acc<VIn>::T) + 4) + (size_t(1) << NBB) * 2 +
-         (size_t(1) << NBB) / 32 * 4 + ((size_t(CAP) * 2 + 15) & ~size_t(15)) + sizeof(cas::StageB<VIn>);
+  return size_t(CAP) * (sizeof(typename cas::Acc<VIn>::T) + 4) + (size_t(1) << NBB) * 2 + size_t(CAP / 32) * 4 +
+         ((size_t(CAP) + 15) & ~size_t(15)) + sizeof(cas::StageB<VIn>);
 }
 
 // symbolic hash shape of each symbolic bin: threads, log2(table slots), byte
@@ -171,7 +171,7 @@ constexpr size_t smem_numc_esc_msd() {
   X(kSB_H32K, 512, 15, 16384)
 
 // bucketed ESC shape of each ESC bin: capacity and log2(bucket count), two to
-// four products per bucket; shared memory allows 8, 6, 4, 3, 3, 2, 1 CTAs of
+// four products per bucket; shared memory allows 8, 7, 4, 3, 3, 2, 1 CTAs of
 // 256 threads per SM for the seven bins
 #define CAS_ESC_SHAPES(X) \
   X(kNB_E1K, 1024, 9)   \

@@ -729,21 +729,135 @@ k_symb_hash(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t* __restrict_
   if (threadIdx.x == 0) row_nz[r] = tot;
 }
 
+__device__ __forceinline__ void atomic_add_sh(double* p, double v) { atomicAdd(p, v); }
+__device__ __forceinline__ void atomic_add_sh(long long* p, long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
+}
+
+// Sorts the (key, value) pairs of one bucket [s, e), 1 <= e - s <= 8, in
+// shared memory by key with the 8-input network in registers, sums equal
+// keys, and leaves the distinct (key, sum) pairs at [s, s + heads) and
+// kEmptyKey behind them; returns heads.  One lane per bucket.
+template <typename AT>
+__device__ __forceinline__ int sort_compact_small(uint32_t* __restrict__ skey, AT* __restrict__ sval, int s, int e) {
+  const int nb = e - s;
+  uint32_t k[8], q[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    k[i] = i < nb ? skey[s + i] : 0xFFFFFFFFu;
+    q[i] = (uint32_t)i;
+  }
+  sort8(k, q);
+  AT v[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = i < nb ? sval[s + q[i]] : AT(0);
+  int h = 0;
+  uint32_t prev = k[0];
+  AT acc = v[0];
+#pragma unroll
+  for (int i = 1; i < 8; ++i) {
+    if (i < nb) {
+      if (k[i] != prev) {
+        skey[s + h] = prev;
+        sval[s + h] = acc;
+        ++h;
+        prev = k[i];
+        acc = v[i];
+      } else {
+        acc += v[i];
+      }
+    }
+  }
+  skey[s + h] = prev;
+  sval[s + h] = acc;
+  ++h;
+  for (int i = h; i < nb; ++i) skey[s + i] = kEmptyKey;
+  return h;
+}
+
+// The same for a bucket of 8 < e - s <= 128 pairs, by a whole warp: every
+// pair's rank is counted against the bucket read by broadcast, the pairs are
+// written back in key order, equal keys are summed into their run's first
+// slot with shared-memory atomics, and the tail is marked kEmptyKey.
+template <typename AT>
+__device__ __forceinline__ int warp_sort_compact(uint32_t* __restrict__ skey, AT* __restrict__ sval, int s, int e) {
+  constexpr int PER = 4;
+  const int lane = threadIdx.x & 31;
+  const int b = e - s;
+  uint32_t k[PER];
+  AT v[PER];
+  int rk[PER];
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    const int idx = lane + 32 * i;
+    k[i] = idx < b ? skey[s + idx] : kEmptyKey;
+    v[i] = idx < b ? sval[s + idx] : AT(0);
+    rk[i] = 0;
+  }
+  for (int j = 0; j < b; ++j) {
+    const uint32_t kj = skey[s + j];
+#pragma unroll
+    for (int i = 0; i < PER; ++i) rk[i] += (kj < k[i]) || (kj == k[i] && j < lane + 32 * i);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    if (lane + 32 * i < b) {
+      skey[s + rk[i]] = k[i];
+      sval[s + rk[i]] = v[i];
+    }
+  }
+  __syncwarp();
+  int heads = 0;
+  int run[PER];
+  bool hd[PER];
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    const int t = lane + 32 * i;
+    k[i] = t < b ? skey[s + t] : kEmptyKey;
+    v[i] = t < b ? sval[s + t] : AT(0);
+    const uint32_t kp = (t > 0 && t < b) ? skey[s + t - 1] : ~k[i];
+    hd[i] = t < b && k[i] != kp;
+    const unsigned m = __ballot_sync(kFull, hd[i]);
+    run[i] = heads + __popc(m & ((lanemask_lt() << 1) | 1u)) - 1;
+    heads += __popc(m);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    if (hd[i]) {
+      skey[s + run[i]] = k[i];
+      sval[s + run[i]] = AT(0);
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < PER; ++i)
+    if (lane + 32 * i < b) atomic_add_sh(&sval[s + run[i]], v[i]);
+  for (int t = heads + lane; t < b; t += 32) skey[s + t] = kEmptyKey;
+  __syncwarp();
+  return heads;
+}
+
 // ESC accumulator with a one-pass bucket sort, for rows of at most CAP
-// products (ams_hsersc_numc_krnl, src/ams/ams_utils.c:399-456): expand
-// (column, a*b) into shared memory while histogramming the products into
-// NB = 2^NBB buckets (about four products per bucket) by the high bits of
-// (column - min column); scatter product indices into bucket order; sort each
-// bucket — one lane per bucket, an 8-input sorting network for the usual
-// buckets of at most 8 products, insertion sort beyond; then sum runs of equal
-// columns, 32 sorted entries per warp step so a warp's stores are contiguous.
-// A row with a bucket of more than kBucketLimit products (columns crowded into
-// a narrow range) is appended to `ovf` and left to the radix-sort ESC kernel.
-// The limit counts products, not distinct columns: the diagonal column of
-// A*A^T alone puts |A_i| products into one bucket, and equal keys cost the
-// insertion sort little.  Shared memory: 14 bytes per product plus half a
-// byte per bucket.
-constexpr int kBucketLimit = 96;
+// products (ams_hsersc_numc_krnl, src/ams/ams_utils.c:399-456):
+//  1. a keys-only expansion histograms the products into NB = 2^NBB buckets
+//     (about four products per bucket) by the high bits of (column - min
+//     column);
+//  2. a second expansion writes every (column, a*b) straight to its bucket's
+//     next slot, so the pairs land in bucket order with no index array;
+//  3. one lane per bucket sorts the bucket by column, sums equal columns and
+//     compacts them to the bucket's front (kEmptyKey behind); buckets of more
+//     than 8 pairs are sorted by a whole warp each;
+//  4. 32 slots at a time, warps count and then write the distinct pairs, so a
+//     warp's global stores are contiguous.
+// A row with a bucket of more than kBucketLimit products (columns crowded
+// into a narrow range) is appended to `ovf` and left to the radix-sort ESC
+// kernel.  The limit counts products, not distinct columns: the diagonal
+// column of A*A^T alone puts |A_i| products into one bucket.  Shared memory:
+// 13 bytes per product plus half a byte per bucket.
+constexpr int kBucketLimit = 128;
+constexpr int kBigBuckets = 64;  // buckets of more than 8 pairs one row may have
 
 template <int BLOCK, int CAP, int NBB, typename VIn>
 __global__ void __launch_bounds__(BLOCK)
@@ -754,24 +868,24 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   constexpr int NB = 1 << NBB;
   constexpr int NW = BLOCK / 32;
   constexpr int NG = NB / 32;
+  constexpr int NCH = CAP / 32;
   constexpr int ACH = BLOCK < kBChunk ? BLOCK : kBChunk;
   static_assert(kBChunk <= 256, "8-bit A entry indices");
-  static_assert(CAP <= 32768 && CAP % 32 == 0, "16-bit indices and counters");
-  static_assert(NG <= BLOCK && NB % (2 * BLOCK) == 0, "one group count per thread; whole counter words per thread");
+  static_assert(CAP <= 32768 && CAP % 32 == 0, "16-bit counters");
+  static_assert(NG <= BLOCK && NCH <= BLOCK && NB % (2 * BLOCK) == 0, "one count per thread in the scans");
   extern __shared__ __align__(16) uint8_t smem[];
   AT* sval = reinterpret_cast<AT*>(smem);
   uint32_t* skey = reinterpret_cast<uint32_t*>(sval + CAP);
-  uint32_t* bcnt = skey + CAP;                 // NB 16-bit counters
-  uint32_t* gcnt = bcnt + NB / 2;              // NG group counts / offsets
-  uint16_t* perm = reinterpret_cast<uint16_t*>(gcnt + NG);
-  uint8_t* segof = reinterpret_cast<uint8_t*>(perm);  // used only while expanding, before perm is written
-  StageB<VIn>& sg = *reinterpret_cast<StageB<VIn>*>(reinterpret_cast<uint8_t*>(perm) + ((CAP * 2 + 15) & ~15));
+  uint32_t* bcnt = skey + CAP;        // NB 16-bit counters
+  uint32_t* ccnt = bcnt + NB / 2;     // NCH chunk counts / offsets
+  uint8_t* segof = reinterpret_cast<uint8_t*>(ccnt + NCH);
+  StageB<VIn>& sg = *reinterpret_cast<StageB<VIn>*>(segof + ((CAP + 15) & ~15));
   const int64_t r = rows[blockIdx.x];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t as = A.rp[r], ae = A.rp[r + 1];
   if (threadIdx.x == 0) { sg.kmin = 0xFFFFFFFFu; sg.kmax = 0u; sg.over = 0; }
   for (int i = threadIdx.x; i < NB / 2; i += BLOCK) bcnt[i] = 0u;
-  // the column range first: from the staged chunk when the row has one chunk,
+  // the column range: from the staged chunk when the row has one chunk,
   // else from a pass over all its A entries (or [0, num_col) when B is unsorted)
   const bool one_chunk = ae - as <= ACH;
   if (!one_chunk) {
@@ -801,130 +915,135 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
     sg.kmax = (uint32_t)(B.ncol > 0 ? B.ncol - 1 : 0);
   }
   __syncthreads();
-  int n = 0;
+  // pass 1: keys only, bucket histogram
+  int n = 0, total = 0;
+  uint32_t lo = 0;
+  int shift = 0;
   for (int64_t a0 = as; a0 < ae; a0 += ACH) {
     const int na = (int)((ae - a0) < (int64_t)ACH ? (ae - a0) : (int64_t)ACH);
-    const int total = stage_chunk<BLOCK, true, VIn>(A, B, a0, na, sg, segof, CAP - n, one_chunk && b_sorted);
+    total = stage_chunk<BLOCK, true, VIn>(A, B, a0, na, sg, segof, CAP - n, one_chunk && b_sorted);
     if (n + total > CAP) {  // uniform: the bin bound was violated
       if (threadIdx.x == 0) dev_report(st, kDevCapacity, 14, r);
       return;
     }
-    const uint32_t lo = sg.kmin, range = sg.kmax - sg.kmin;
-    const int bits = (sg.kmax > sg.kmin) ? 32 - __clz(range) : 0;
-    const int shift = bits > NBB ? bits - NBB : 0;
-    const int base = n;
-    expand_chunk<BLOCK, true, VIn>(B, total, sg, segof, [&](int32_t key, VIn av, VIn bv, int p) {
-      skey[base + p] = (uint32_t)key;
-      sval[base + p] = Acc<VIn>::mul(av, bv);
+    lo = sg.kmin;
+    const int bits = (sg.kmax > sg.kmin) ? 32 - __clz(sg.kmax - sg.kmin) : 0;
+    shift = bits > NBB ? bits - NBB : 0;
+    expand_chunk<BLOCK, false, VIn>(B, total, sg, segof, [&](int32_t key, VIn, VIn, int) {
       bucket_add(bcnt, (int)(((uint32_t)key - lo) >> shift));
     });
     n += total;
-    __syncthreads();
+    if (!one_chunk) __syncthreads();
   }
-  const uint32_t lo = sg.kmin, range = sg.kmax - sg.kmin;
-  const int bits = (sg.kmax > sg.kmin) ? 32 - __clz(range) : 0;
-  const int shift = bits > NBB ? bits - NBB : 0;
+  __syncthreads();
   // exclusive scan of the bucket counts: NB / BLOCK consecutive buckets per thread
   constexpr int WPT = NB / (2 * BLOCK);
-  uint32_t loc[WPT];
-  uint32_t sum = 0, big = 0;
+  {
+    uint32_t loc[WPT];
+    uint32_t sum = 0, big = 0;
 #pragma unroll
-  for (int i = 0; i < WPT; ++i) {
-    loc[i] = bcnt[threadIdx.x * WPT + i];
-    const uint32_t c0 = loc[i] & 0xFFFFu, c1 = loc[i] >> 16;
-    sum += c0 + c1;
-    big = max(big, max(c0, c1));
-  }
-  if (__syncthreads_or(big > (uint32_t)kBucketLimit)) {
-    if (threadIdx.x == 0) ovf[atomicAdd(ovf_count, 1u)] = (int32_t)r;
-    return;
-  }
-  int tot_all;
-  uint32_t run = (uint32_t)block_exclusive_sum<BLOCK, int>((int)sum, sg.tmp, tot_all);
+    for (int i = 0; i < WPT; ++i) {
+      loc[i] = bcnt[threadIdx.x * WPT + i];
+      const uint32_t c0 = loc[i] & 0xFFFFu, c1 = loc[i] >> 16;
+      sum += c0 + c1;
+      big = max(big, max(c0, c1));
+    }
+    if (__syncthreads_or(big > (uint32_t)kBucketLimit)) {
+      if (threadIdx.x == 0) ovf[atomicAdd(ovf_count, 1u)] = (int32_t)r;
+      return;
+    }
+    int tot_all;
+    uint32_t run = (uint32_t)block_exclusive_sum<BLOCK, int>((int)sum, sg.tmp, tot_all);
 #pragma unroll
-  for (int i = 0; i < WPT; ++i) {
-    const uint32_t c0 = loc[i] & 0xFFFFu, c1 = loc[i] >> 16;
-    bcnt[threadIdx.x * WPT + i] = run | ((run + c0) << 16);
-    run += c0 + c1;
+    for (int i = 0; i < WPT; ++i) {
+      const uint32_t c0 = loc[i] & 0xFFFFu, c1 = loc[i] >> 16;
+      bcnt[threadIdx.x * WPT + i] = run | ((run + c0) << 16);
+      run += c0 + c1;
+    }
   }
   __syncthreads();
-  // scatter product indices into bucket order; bucket b then ends at bucket_get(b)
-  for (int p = threadIdx.x; p < n; p += BLOCK) perm[bucket_add(bcnt, (int)((skey[p] - lo) >> shift))] = (uint16_t)p;
+  // pass 2: (column, a*b) straight into bucket order; bucket b then ends at bucket_get(b)
+  if (one_chunk) {
+    expand_chunk<BLOCK, true, VIn>(B, total, sg, segof, [&](int32_t key, VIn av, VIn bv, int) {
+      const int pos = (int)bucket_add(bcnt, (int)(((uint32_t)key - lo) >> shift));
+      skey[pos] = (uint32_t)key;
+      sval[pos] = Acc<VIn>::mul(av, bv);
+    });
+  } else {
+    int m = 0;
+    for (int64_t a0 = as; a0 < ae; a0 += ACH) {
+      const int na = (int)((ae - a0) < (int64_t)ACH ? (ae - a0) : (int64_t)ACH);
+      const int t = stage_chunk<BLOCK, true, VIn>(A, B, a0, na, sg, segof, CAP - m, false);
+      expand_chunk<BLOCK, true, VIn>(B, t, sg, segof, [&](int32_t key, VIn av, VIn bv, int) {
+        const int pos = (int)bucket_add(bcnt, (int)(((uint32_t)key - lo) >> shift));
+        skey[pos] = (uint32_t)key;
+        sval[pos] = Acc<VIn>::mul(av, bv);
+      });
+      m += t;
+      __syncthreads();
+    }
+  }
   __syncthreads();
-  // one lane per bucket: sort it by column, count its distinct columns
+  // sort each bucket, sum equal columns, compact them to the bucket front:
+  // one lane per bucket of at most 8 pairs; larger buckets (about 1 in 100,
+  // and the diagonal column's) are queued for a whole warp each
+  __shared__ uint16_t s_big[kBigBuckets];
+  __shared__ int s_nbig;
+  if (threadIdx.x == 0) s_nbig = 0;
+  __syncthreads();
   for (int g = warp; g < NG; g += NW) {
     const int b = g * 32 + lane;
     const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
-    const int nb = e - s;
-    int heads;
-    if (nb <= 8) {
-      uint32_t k[8], q[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        q[i] = i < nb ? perm[s + i] : 0u;
-        k[i] = i < nb ? skey[q[i]] : 0xFFFFFFFFu;
-      }
-      sort8(k, q);
-      heads = nb > 0;
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        if (i < nb) perm[s + i] = (uint16_t)q[i];
-        if (i > 0 && i < nb) heads += k[i] != k[i - 1];
-      }
-    } else {
-      for (int i = s + 1; i < e; ++i) {
-        const uint16_t pi = perm[i];
-        const uint32_t ki = skey[pi];
-        int j = i - 1;
-        while (j >= s && skey[perm[j]] > ki) {
-          perm[j + 1] = perm[j];
-          --j;
-        }
-        perm[j + 1] = pi;
-      }
-      heads = 1;
-      for (int i = s + 1; i < e; ++i) heads += skey[perm[i]] != skey[perm[i - 1]];
+    if (e - s > 8) {
+      const int slot = atomicAdd(&s_nbig, 1);
+      if (slot < kBigBuckets) s_big[slot] = (uint16_t)b;
+    } else if (e > s) {
+      sort_compact_small<AT>(skey, sval, s, e);
     }
-    heads = warp_sum(heads);
-    if (lane == 0) gcnt[g] = (uint32_t)heads;
   }
   __syncthreads();
-  int total;
+  if (s_nbig > kBigBuckets) {  // uniform: too many large buckets for this form
+    if (threadIdx.x == 0) ovf[atomicAdd(ovf_count, 1u)] = (int32_t)r;
+    return;
+  }
+  for (int i = warp; i < s_nbig; i += NW) {
+    const int b = s_big[i];
+    const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
+    warp_sort_compact<AT>(skey, sval, s, e);
+  }
+  __syncthreads();
+  // distinct pairs per 32-slot chunk, then chunk offsets
+  const int nch = (n + 31) >> 5;
+  for (int c = warp; c < nch; c += NW) {
+    const int t = c * 32 + lane;
+    const bool valid = t < n && skey[t] != kEmptyKey;
+    const unsigned m = __ballot_sync(kFull, valid);
+    if (lane == 0) ccnt[c] = __popc(m);
+  }
+  __syncthreads();
+  int distinct;
   {
-    const int c = threadIdx.x < NG ? (int)gcnt[threadIdx.x] : 0;
-    const int ex = block_exclusive_sum<BLOCK, int>(c, sg.tmp, total);
-    if (threadIdx.x < NG) gcnt[threadIdx.x] = (uint32_t)ex;
+    const int cnum = threadIdx.x < nch ? (int)ccnt[threadIdx.x] : 0;
+    const int ex = block_exclusive_sum<BLOCK, int>(cnum, sg.tmp, distinct);
+    if (threadIdx.x < nch) ccnt[threadIdx.x] = (uint32_t)ex;
   }
   __syncthreads();
-  // each group's sorted entries, 32 at a time: run heads write (column, sum)
-  // to consecutive positions.  Equal columns share a bucket, so no run
-  // crosses a group.
   const int64_t c0 = crp[r], nz = crp[r + 1] - c0;
-  for (int g = warp; g < NG; g += NW) {
-    const int gs = g ? (int)bucket_get(bcnt, g * 32 - 1) : 0, ge = (int)bucket_get(bcnt, g * 32 + 31);
-    int64_t out = gcnt[g];
-    for (int e0 = gs; e0 < ge; e0 += 32) {
-      const int t = e0 + lane;
-      bool head = false;
-      uint32_t key = 0;
-      if (t < ge) {
-        key = skey[perm[t]];
-        head = t == gs || key != skey[perm[t - 1]];
+  for (int c = warp; c < nch; c += NW) {
+    const int t = c * 32 + lane;
+    uint32_t key = kEmptyKey;
+    if (t < n) key = skey[t];
+    const bool valid = key != kEmptyKey;
+    const unsigned m = __ballot_sync(kFull, valid);
+    if (valid) {
+      const int64_t pos = (int64_t)ccnt[c] + __popc(m & lanemask_lt());
+      if (pos < nz) {
+        ccol[c0 + pos] = (int32_t)key;
+        cval[c0 + pos] = sval[t];
       }
-      const unsigned hm = __ballot_sync(kFull, head);
-      if (head) {
-        AT v = sval[perm[t]];
-        for (int t2 = t + 1; t2 < ge && skey[perm[t2]] == key; ++t2) v += sval[perm[t2]];
-        const int64_t pos = out + __popc(hm & lanemask_lt());
-        if (pos < nz) {
-          ccol[c0 + pos] = (int32_t)key;
-          cval[c0 + pos] = v;
-        }
-      }
-      out += __popc(hm);
     }
   }
-  if (threadIdx.x == 0 && total != nz) dev_report(st, total > nz ? kDevRowOverflow : kDevRowUnderflow, 14, r);
+  if (threadIdx.x == 0 && distinct != nz) dev_report(st, distinct > nz ? kDevRowOverflow : kDevRowUnderflow, 14, r);
 }
 
 // Hash accumulator for rows with at most 2^TBITS / 2 distinct columns: linear
