@@ -663,8 +663,9 @@ int cas_mtx_write(const char *path, int64_t num_row, int64_t num_col, const int6
 			}
 		}
 	}
-	fprintf(f, symmetric ? "%%%%MatrixMarket matrix coordinate real symmetric\n"
-		: "%%%%MatrixMarket matrix coordinate real general\n");
+	/* the reference's header line has one '%' (its format string is "%%...") */
+	fputs(symmetric ? "%MatrixMarket matrix coordinate real symmetric\n"
+		: "%MatrixMarket matrix coordinate real general\n", f);
 	fprintf(f, "%ld %ld %ld\n", (long) num_row, (long) num_col, (long) cnt);
 	size_t bcap = 1 << 22;
 	char *b = (char *) malloc(bcap + 128);

@@ -11,6 +11,13 @@ tests/test_oracle.py.
 The MatrixMarket fixture pins the loader: `loader_sym.mtx` read by the
 reference's raw2csr (src/mm/mm_utils.c:451-692).
 
+The driver fixtures pin the process boundary: `rmat_ones/` holds a small
+PaRMAT-style edge list and the two files the reference's rmat_ones
+(src/rmat_ones.c) writes from it; `driver_<algo>_g500_12_8.log` is the
+stdout of the reference's ams_<algo>spgemm driver (built with IN_VERIFY) on
+the dataset `bin/cas_gen g500 12 8` writes, whose VERIFYRESULT triple and
+line layout the GPU drivers must reproduce.
+
 Run from the repository root, where oracle/_ref has been built:
     python tests/golden/make_golden.py
 """
@@ -24,6 +31,10 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "contention-aware-spgemm_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+import shutil  # noqa: E402
+import subprocess  # noqa: E402
+import tempfile  # noqa: E402
 
 import casgemm  # noqa: E402
 import oracle  # noqa: E402
@@ -86,5 +97,32 @@ def main():
     print(f"loader_sym: {nr}x{nc} nnz={len(cols)}")
 
 
+def driver_fixtures():
+    ref = os.path.join(ROOT, "oracle", "_ref")
+    gen = os.path.join(ROOT, "contention-aware-spgemm_b200", "bin", "cas_gen")
+    with tempfile.TemporaryDirectory() as tmp:
+        ds = os.path.join(tmp, "dataset")
+        os.makedirs(ds)
+        # edge list: each undirected edge of a seeded R-MAT once, 0-based
+        A = casgemm.gen_g500(4, 2, 5)
+        rows = np.repeat(np.arange(A.num_row), np.diff(A.row_ptrs))
+        keep = rows < A.cols
+        edges = "".join(f"{u}\t{v}\n" for u, v in zip(rows[keep], A.cols[keep]))
+        open(os.path.join(ds, "g500_4_2.txt"), "w").write(edges)
+        subprocess.run([os.path.join(ref, "rmat_ones"), "g500_4_2"], cwd=tmp, check=True, capture_output=True)
+        out = os.path.join(HERE, "rmat_ones")
+        os.makedirs(out, exist_ok=True)
+        for suffix in (".txt", ".org.mtx", ".trs.mtx"):
+            shutil.copy(os.path.join(ds, "g500_4_2" + suffix), os.path.join(out, "g500_4_2" + suffix))
+        subprocess.run([gen, "g500", "12", "8"], cwd=tmp, check=True, capture_output=True,
+                       env=dict(os.environ, CAS_DATASET_DIR=ds))
+        for algo in ("hash", "hsersc", "hybacc"):
+            p = subprocess.run([os.path.join(ref, f"ams_{algo}spgemm"), "g500_12_8"], cwd=tmp, check=True,
+                               capture_output=True, text=True)
+            open(os.path.join(HERE, f"driver_{algo}_g500_12_8.log"), "w").write(p.stdout)
+            print(f"driver_{algo}: {sum(1 for x in p.stdout.splitlines() if x.startswith('VERIFYRESULT'))} verify lines")
+
+
 if __name__ == "__main__":
     main()
+    driver_fixtures()
