@@ -58,6 +58,28 @@ class CasStats(ctypes.Structure):
     ]
 
 
+class CasJob(ctypes.Structure):
+    _fields_ = [
+        ("A", CasCsr), ("B", CasCsr), ("row_digests", ctypes.c_void_p),
+        ("flop", ctypes.c_int64), ("nnz_c", ctypes.c_int64), ("digest", ctypes.c_uint64),
+        ("status", ctypes.c_int32),
+    ]
+
+
+class CasBatchStats(ctypes.Structure):
+    _fields_ = [
+        ("seconds", ctypes.c_double), ("waves", ctypes.c_int64), ("jobs_ok", ctypes.c_int64),
+        ("flop", ctypes.c_int64), ("nnz_c", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
+        ("h2d_bytes", ctypes.c_double), ("max_wave_bound", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+BATCH_MODES = {"waves": 0, "per_call": 1}
+
+
 class CasError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"{STATUS.get(status, status)}: {msg}")
@@ -87,6 +109,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "cas_spgemm": (I32, [P, I32, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr),
                              ctypes.POINTER(CasRuntime)]),
         "cas_csr_free": (I32, [P, ctypes.POINTER(CasCsr)]),
+        "cas_csr_digest": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(ctypes.c_uint64), P]),
+        "cas_batch_run": (I32, [P, I32, ctypes.POINTER(CasJob), I64, I32, D, ctypes.POINTER(CasBatchStats)]),
         "cas_flp_populate": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), P]),
         "cas_scan": (I32, [P, P, P, I64]),
         "cas_hash_symb": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), P, P]),
@@ -261,6 +285,45 @@ class Context:
     def free(self, cc: CasCsr):
         self._check(self.lib.cas_csr_free(self.h, ctypes.byref(cc)))
 
+    def digest(self, cc: CasCsr, rows: bool = False):
+        """Digest of a device CSR (cas_csr_digest); with rows, also its row digests."""
+        d = ctypes.c_uint64()
+        rd = np.empty(cc.num_row, np.uint64) if rows else None
+        self._check(self.lib.cas_csr_digest(self.h, ctypes.byref(cc), ctypes.byref(d), _ptr(rd)))
+        return (int(d.value), rd) if rows else int(d.value)
+
+    def batch_run(self, jobs, accum: str = "hybacc", mode: str = "waves", wave_budget: float = 0.0,
+                  row_digests: bool = False):
+        """Independent products C_j = A_j * B_j (cas_batch_run).
+
+        jobs: list of (A, B), each a host Csr or a DeviceCsr.  Returns (per-job
+        dicts with flop, nnz_c, digest, status and optionally row_digests,
+        batch stats)."""
+        arr = (CasJob * max(1, len(jobs)))()
+        keep = []
+        rds = []
+        for j, (A, B) in enumerate(jobs):
+            ca = A.as_cas() if isinstance(A, Csr) else A.c
+            cb = B.as_cas() if isinstance(B, Csr) else B.c
+            keep.append((A, B))
+            arr[j].A, arr[j].B = ca, cb
+            rd = np.zeros(ca.num_row, np.uint64) if row_digests else None
+            rds.append(rd)
+            arr[j].row_digests = _ptr(rd) if rd is not None and len(rd) else None
+        st = CasBatchStats()
+        rc = self.lib.cas_batch_run(self.h, ACCUM[accum], arr, len(jobs), BATCH_MODES[mode], float(wave_budget),
+                                    ctypes.byref(st))
+        out = []
+        for j in range(len(jobs)):
+            d = {"flop": arr[j].flop, "nnz_c": arr[j].nnz_c, "digest": int(arr[j].digest),
+                 "status": arr[j].status}
+            if row_digests:
+                d["row_digests"] = rds[j]
+            out.append(d)
+        if rc != 0:
+            raise CasError(rc, self.lib.cas_last_error(self.h).decode())
+        return out, st.as_dict()
+
 
 # ---------------------------------------------------------------- data layer
 def gen_rmat(scale: int, edge_factor: int, a: float, b: float, c: float, seed: int) -> Csr:
@@ -374,3 +437,34 @@ def slice_rows(A: Csr, r0: int, r1: int) -> Csr:
     """Rows [r0, r1) of A as a CSR of its own (views, no copy of columns/values)."""
     s, e = int(A.row_ptrs[r0]), int(A.row_ptrs[r1])
     return Csr(r1 - r0, A.num_col, A.row_ptrs[r0:r1 + 1] - s, A.cols[s:e], A.vals[s:e])
+
+
+# ------------------------------------------------------------ batch workload
+def _splitmix(x: int) -> int:
+    x = (x + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+    x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+    x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+    return x ^ (x >> 31)
+
+
+def batch_spec(n: int = 512, seed: int = 4, scales=(10, 17), edge_factors=(2, 4, 8, 16, 32)):
+    """The uneven batch: job j is a G500 R-MAT with scale uniform in
+    [scales[0], scales[1]] and edge factor uniform over edge_factors, drawn
+    from (seed, j) by SplitMix64; returns [(scale, edge_factor, graph_seed)]."""
+    out = []
+    span = scales[1] - scales[0] + 1
+    for j in range(n):
+        base = _splitmix((seed << 32) ^ j)
+        s = scales[0] + _splitmix(base ^ 1) % span
+        ef = edge_factors[_splitmix(base ^ 2) % len(edge_factors)]
+        out.append((int(s), int(ef), int(_splitmix(base ^ 3) & 0xFFFFFFFF)))
+    return out
+
+
+def batch_job(scale: int, edge_factor: int, graph_seed: int, int_vals: bool = True):
+    """One job of the batch: (A, B = A^T) with int32 values uniform in 1..8
+    (accumulated in int64), or values 1.0."""
+    A = gen_g500(scale, edge_factor, graph_seed)
+    if int_vals:
+        A = Csr(A.num_row, A.num_col, A.row_ptrs, A.cols, int_values(A.nnz, graph_seed ^ 0x5DEECE66D))
+    return A, transpose(A)

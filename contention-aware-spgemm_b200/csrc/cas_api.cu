@@ -507,7 +507,8 @@ cas_status launch_symb_bins(cas_ctx* ctx, Call& c, int64_t* row_nz) {
       case kSB_Dense:
         if (!c.b_sorted && c.ncol > kDenseChunkBits)
           return set_err(ctx, CAS_ERR_BAD_INPUT, "heavy rows over more than %d columns need B rows sorted by column", kDenseChunkBits);
-        k_symb_dense<1024><<<(unsigned)n, 1024, smem_symb_dense<1024>(), s>>>(rows, c.A.csr, c.B.csr, c.ncol, row_nz, ctx->d_status);
+        k_symb_dense<1024><<<(unsigned)n, 1024, smem_symb_dense<1024>(), s>>>(rows, c.A.csr, c.B.csr, c.ncol,
+                                                                            c.b_sorted ? 1 : 0, row_nz, ctx->d_status);
         break;
     }
     CAS_TRY(check_launch(ctx, "symbolic bin"));
@@ -598,7 +599,8 @@ cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* 
       case kNB_Dense:
         if (!c.b_sorted && c.ncol > kDenseChunkCols)
           return set_err(ctx, CAS_ERR_BAD_INPUT, "heavy rows over more than %d columns need B rows sorted by column", kDenseChunkCols);
-        k_numc_dense<1024, VIn><<<(unsigned)n, 1024, smem_numc_dense<1024, VIn>(), s>>>(rows, A, B, c.ncol, crp, ccol, cval, ctx->d_status);
+        k_numc_dense<1024, VIn><<<(unsigned)n, 1024, smem_numc_dense<1024, VIn>(), s>>>(
+            rows, A, B, c.ncol, c.b_sorted ? 1 : 0, crp, ccol, cval, ctx->d_status);
         break;
     }
     CAS_TRY(check_launch(ctx, "numeric bin"));
@@ -987,6 +989,9 @@ cas_status cas_hybacc_numc(cas_ctx* ctx, const cas_csr* A, const cas_csr* B, con
 }
 
 }  // extern "C"
+
+// ============================================= digests and batches of products
+#include "cas_batch.cu"
 
 // ===================================================== scan without allocation
 // cas_scan_noalloc: the same exclusive scan as cas_scan, for callers that must

@@ -314,22 +314,65 @@ k_symb_tiny(const int32_t* __restrict__ rows, int64_t nrows, Csr A, Csr B, int64
   if (lane == 0) row_nz[r] = cnt;
 }
 
-// Heavy rows: a bitmap over kDenseChunkBits columns at a time; the count is
-// the population count.  B rows are cut to each column chunk by binary search
-// when there is more than one chunk.
+// Column range [lo, hi) that row r of A*B can reach: with B's rows sorted,
+// from the first and last column of every B row the row gathers; otherwise
+// [0, ncol).  Block-wide; every thread gets the range.
+template <int BLOCK>
+__device__ __forceinline__ void row_col_range(const Csr& A, const Csr& B, int64_t r, bool b_sorted, int64_t ncol,
+                                              int64_t& lo, int64_t& hi) {
+  __shared__ uint32_t red[2];
+  if (!b_sorted) {
+    lo = 0;
+    hi = ncol;
+    return;
+  }
+  if (threadIdx.x == 0) { red[0] = 0xFFFFFFFFu; red[1] = 0u; }
+  __syncthreads();
+  uint32_t mn = 0xFFFFFFFFu, mx = 0u;
+  const int64_t ae = A.rp[r + 1];
+  for (int64_t j = A.rp[r] + threadIdx.x; j < ae; j += BLOCK) {
+    const int32_t k = A.col[j];
+    const int64_t s = B.rp[k], e = B.rp[k + 1];
+    if (e > s) {
+      mn = min(mn, (uint32_t)__ldg(B.col + s));
+      mx = max(mx, (uint32_t)__ldg(B.col + e - 1));
+    }
+  }
+  mn = warp_min_u32(mn);
+  mx = warp_max_u32(mx);
+  if ((threadIdx.x & 31) == 0 && mx >= mn) {
+    atomicMin(&red[0], mn);
+    atomicMax(&red[1], mx);
+  }
+  __syncthreads();
+  if (red[1] >= red[0]) {
+    lo = red[0];
+    hi = (int64_t)red[1] + 1;
+  } else {
+    lo = hi = 0;
+  }
+  __syncthreads();
+}
+
+// Heavy rows: a bitmap over kDenseChunkBits columns at a time, one pass per
+// chunk of the row's column range; the count is the population count.  B
+// rows are cut to each column chunk by binary search when there is more than
+// one chunk.
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
-k_symb_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int64_t* __restrict__ row_nz,
-             DevStatus* st) {
+k_symb_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int32_t b_sorted,
+             int64_t* __restrict__ row_nz, DevStatus* st) {
   constexpr int W = kDenseChunkBits / 32;
   extern __shared__ __align__(16) uint8_t smem[];
   uint32_t* bm = reinterpret_cast<uint32_t*>(smem);
   Stage<double>& sg = *reinterpret_cast<Stage<double>*>(smem + W * sizeof(uint32_t));
   const int64_t r = rows[blockIdx.x];
-  const bool multi = c_ncol > kDenseChunkBits;
+  int64_t lo, hi;
+  row_col_range<BLOCK>(A, B, r, b_sorted != 0, c_ncol, lo, hi);
+  const bool multi = hi - lo > kDenseChunkBits;
   long long cnt = 0;
-  for (int64_t c0 = 0; c0 < c_ncol; c0 += kDenseChunkBits) {
-    const int64_t c1 = (c_ncol < c0 + kDenseChunkBits ? c_ncol : c0 + kDenseChunkBits);
+  for (int64_t c0 = lo; c0 < hi; c0 += kDenseChunkBits) {
+    const int64_t c1 = (hi < c0 + kDenseChunkBits ? hi : c0 + kDenseChunkBits);
     for (int i = threadIdx.x; i < W; i += BLOCK) bm[i] = 0u;
     __syncthreads();
     bool bad = false;
@@ -1136,8 +1179,9 @@ k_numc_hash(const int32_t* __restrict__ rows, Csr A, Csr B, const int64_t* __res
 // chunk by binary search (B rows sorted by column).
 template <int BLOCK, typename VIn>
 __global__ void __launch_bounds__(BLOCK)
-k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, const int64_t* __restrict__ crp,
-             int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval, DevStatus* st) {
+k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int32_t b_sorted,
+             const int64_t* __restrict__ crp, int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval,
+             DevStatus* st) {
   using AT = typename Acc<VIn>::T;
   constexpr int CW = kDenseChunkCols;
   constexpr int NWORD = CW / 32;
@@ -1148,10 +1192,12 @@ k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, con
   Stage<VIn>& sg = *reinterpret_cast<Stage<VIn>*>(reinterpret_cast<uint8_t*>(bm + NWORD));
   const int64_t r = rows[blockIdx.x];
   const int64_t c0r = crp[r], nz = crp[r + 1] - c0r;
-  const bool multi = c_ncol > CW;
+  int64_t lo, hi;
+  row_col_range<BLOCK>(A, B, r, b_sorted != 0, c_ncol, lo, hi);
+  const bool multi = hi - lo > CW;
   int64_t written = 0;
-  for (int64_t c0 = 0; c0 < c_ncol; c0 += CW) {
-    const int64_t c1 = (c_ncol < c0 + CW ? c_ncol : c0 + CW);
+  for (int64_t c0 = lo; c0 < hi; c0 += CW) {
+    const int64_t c1 = (hi < c0 + CW ? hi : c0 + CW);
     for (int i = threadIdx.x; i < CW; i += BLOCK) dv[i] = AT(0);
     for (int i = threadIdx.x; i < NWORD; i += BLOCK) bm[i] = 0u;
     __syncthreads();

@@ -161,6 +161,63 @@ cas_status cas_spgemm(cas_ctx *ctx, cas_accum accum, const cas_csr *A, const cas
 /* Frees arrays the library allocated (owned != 0) and zeroes the struct. */
 cas_status cas_csr_free(cas_ctx *ctx, cas_csr *C);
 
+/* ---- digests of a product ------------------------------------------------
+ *
+ * A 64-bit digest of a CSR C that depends on every row's entries in order,
+ * so two products agree bit for bit if their digests do (up to collisions):
+ *   h(c, k, v) = mix64(c * 0x9E3779B97F4A7C15 + k) ^ mix64(bits(v) + 0x632BE59BD9B4E019)
+ *   row_digest[r] = sum over the row's entries, k = 0, 1, ... of h(col_k, k, val_k)
+ *   digest = sum over rows r of mix64(row_digest[r] + r)
+ * all sums modulo 2^64; mix64 is the SplitMix64 finaliser (Steele, Lea,
+ * Flood 2014); bits(v) is the fp64 bit pattern, or the int64 value for
+ * CAS_VAL_I32 outputs.  No counterpart in the reference, whose IN_VERIFY
+ * build prints nnz, the sum of columns and the sum of values
+ * (src/ams_hashspgemm.c:307-318). */
+cas_status cas_csr_digest(cas_ctx *ctx, const cas_csr *C, uint64_t *digest, uint64_t *row_digests);
+
+/* ---- batches of independent products -------------------------------------
+ *
+ * No counterpart in the reference, which runs one product per process.  A
+ * batch runs many independent products C_j = A_j * B_j of uneven sizes on
+ * one device.  Outputs are not kept: each job reports its product count,
+ * nnz(C_j), the digest above, and per-row digests when row_digests is set
+ * (a host array of A_j.num_row entries). */
+typedef struct {
+	cas_csr A, B;            /* inputs: host or device (col_bytes 4), one value type per batch */
+	uint64_t *row_digests;   /* optional host output, A.num_row entries */
+	int64_t flop;            /* out: intermediate products */
+	int64_t nnz_c;           /* out */
+	uint64_t digest;         /* out */
+	int32_t status;          /* out: cas_status of the job */
+} cas_job;
+
+typedef enum {
+	/* All jobs as one block-diagonal product diag(A_j) * diag(B_j): the
+	 * inputs are packed into one device CSR pair (columns shifted per job), the
+	 * rows run in waves that fit wave_budget bytes of output by the bound
+	 * 12 * min(products, columns) per row, and each wave's bins launch once
+	 * over the rows of every job in it. */
+	CAS_BATCH_WAVES = 0,
+	/* One cas_spgemm per job, in order: the same kernels, launched per job. */
+	CAS_BATCH_PER_CALL = 1
+} cas_batch_mode;
+
+typedef struct {
+	double seconds;          /* device time from the first copy to the last digest (CUDA events) */
+	int64_t waves;           /* products run (waves, or jobs for PER_CALL) */
+	int64_t jobs_ok;
+	int64_t flop;            /* sum over jobs */
+	int64_t nnz_c;           /* sum over jobs */
+	int64_t kernel_launches; /* library kernels launched by the batch */
+	double h2d_bytes;
+	double max_wave_bound;   /* largest wave's output bound, bytes */
+} cas_batch_stats;
+
+/* Runs the batch; wave_budget <= 0 means 32 GiB.  Returns CAS_OK when every
+ * job succeeded, else the first failure (each job's status says which). */
+cas_status cas_batch_run(cas_ctx *ctx, cas_accum accum, cas_job *jobs, int64_t n, cas_batch_mode mode,
+	double wave_budget, cas_batch_stats *stats);
+
 /* ---- scan that allocates nothing ---------------------------------------- */
 
 /* The exclusive scan of cas_scan (d_out[0] = 0, d_out[i+1] = d_out[i] +

@@ -181,3 +181,42 @@ def ref_info(algo: str = "hybacc", small: bool = False) -> dict:
 
 def oracle_lib():
     return _load_oracle()
+
+
+# ------------------------------------------------------------------ digests
+_M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def _mix64(z: np.ndarray) -> np.ndarray:
+    """SplitMix64 finaliser (Steele, Lea, Flood 2014) on uint64 arrays (mod 2^64)."""
+    with np.errstate(over="ignore"):
+        z = z + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def csr_digest(rp, cols, vals):
+    """The product digest of the casgemm ABI (cas_csr_digest), restated in numpy.
+
+    Entry k of row r with column c and value v hashes to
+    mix64(c * 0x9E3779B97F4A7C15 + k) ^ mix64(bits(v) + 0x632BE59BD9B4E019);
+    a row's digest is the sum of its entries' hashes, and the product's is the
+    sum over rows of mix64(row digest + r), all mod 2^64.  Returns
+    (digest, row digests)."""
+    rp = np.asarray(rp, np.int64)
+    m = len(rp) - 1
+    cols = np.asarray(cols).astype(np.int64).view(np.uint64)
+    v = np.asarray(vals)
+    bits = v.view(np.uint64) if v.dtype == np.float64 else v.astype(np.int64).view(np.uint64)
+    row = np.repeat(np.arange(m, dtype=np.int64), np.diff(rp))
+    k = (np.arange(len(cols), dtype=np.int64) - rp[:-1][row]).view(np.uint64)
+    with np.errstate(over="ignore"):
+        h = _mix64(cols * np.uint64(0x9E3779B97F4A7C15) + k) ^ _mix64(bits + np.uint64(0x632BE59BD9B4E019))
+        rows = np.zeros(m, np.uint64)
+        np.add.at(rows, row, h)
+        d = _mix64(rows + np.arange(m, dtype=np.uint64))
+        total = np.uint64(0)
+        for chunk in np.array_split(d, max(1, len(d) // 65536)):
+            total = total + np.add.reduce(chunk, dtype=np.uint64)
+    return int(total), rows
