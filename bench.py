@@ -278,10 +278,111 @@ def run_batch_mode(args):
     return 0
 
 
+def serve_pool(n_pool, seed):
+    """Distinct requests of the serving stream: half G500 R-MAT (scale
+    uniform in [12, 19], edge factor uniform in 4..32), half Zipf bipartite
+    (rows log-uniform in [10k, 500k], 2.35 columns per row as in the 850k x
+    2M join-aggregate set, row law Zipf(1.2) with the largest row scaled
+    from 50,000 at 850k rows, column law Zipf(1.4) shifted by q_c = 1000,
+    average degree uniform in [8, 24]); values 1.0."""
+    import casgemm
+    rng = np.random.default_rng(seed)
+    pool = []
+    for i in range(n_pool):
+        if i % 2 == 0:
+            s = int(round(rng.uniform(12, 19)))
+            ef = int(rng.integers(4, 33))
+            A = casgemm.gen_g500(s, ef, int(rng.integers(1 << 31)))
+            name = f"g500_s{s}_ef{ef}"
+        else:
+            nr = int(round(np.exp(rng.uniform(np.log(1e4), np.log(5e5)))))
+            nc = int(2.35 * nr)
+            deg = float(rng.uniform(8, 24))
+            amax = int(min(nc, max(deg * 4, 50000 * nr / 850000)))
+            A = casgemm.gen_zipf(nr, nc, amax, int(deg * nr), int(rng.integers(1 << 31)), col_q=1000.0)
+            name = f"zipf_{nr}x{nc}_d{deg:.0f}"
+        pool.append((name, A, A.transpose()))
+    return pool
+
+
+def run_serve_mode(args):
+    """Serving stream: Poisson arrivals at --rate requests/s, requests drawn
+    from a pool of distinct matrices, admitted by the 60 GB bound; p50/p99
+    latency (completion - arrival) and jobs/s.  Every result's digest must
+    equal the digest of the same request run alone."""
+    import threading
+    import casgemm
+    t0 = time.time()
+    pool = serve_pool(args.pool, 5)
+    log(f"generated a pool of {len(pool)} requests in {time.time() - t0:.1f}s")
+    # alone: each distinct request by itself on a one-slot server
+    solo = {}
+    with casgemm.Server(slots=1) as srv:
+        for k, (name, A, B) in enumerate(pool):
+            r = srv.wait(srv.submit(A, B))
+            if r["status"] != 0:
+                raise RuntimeError(f"{name}: status {r['status']}")
+            solo[k] = (r["digest"], r["nnz_c"], r["flop"], r["t_done"] - r["t_admit"])
+    rng = np.random.default_rng(55)
+    picks = rng.integers(0, len(pool), args.requests)
+    gaps = rng.exponential(1.0 / args.rate, args.requests)
+    sampler = ClockSampler(gpu_index(0))
+    sampler.start()
+    ids = [None] * args.requests
+    with casgemm.Server(slots=args.slots, mem_budget=60e9) as srv:
+        start = srv.clock()
+
+        def feeder():
+            t = start
+            for i in range(args.requests):
+                t += gaps[i]
+                d = t - srv.clock()
+                if d > 0:
+                    time.sleep(d)
+                _, A, B = pool[picks[i]]
+                ids[i] = srv.submit(A, B)
+
+        th = threading.Thread(target=feeder)
+        th.start()
+        th.join()
+        res = [srv.wait(i) for i in ids]
+        st = srv.stats()
+    clocks = sampler.stop()
+    bad = [i for i, r in enumerate(res) if r["status"] != 0 or (r["digest"], r["nnz_c"]) != solo[picks[i]][:2]]
+    if bad:
+        raise RuntimeError(f"{len(bad)} results differ from the same request alone (first: {bad[0]})")
+    lat = np.array([r["t_done"] - r["t_submit"] for r in res])
+    span = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
+    flop = sum(r["flop"] for r in res)
+    line = {
+        "metric": "SpGEMM serving: jobs/s with p50/p99 latency (continuous batching, 60 GB admission budget)",
+        "value": round(args.requests / span, 3), "unit": "jobs/s", "n_gpus": 1, "steps": args.requests,
+        "warmup": len(pool), "ms_per_step": round(1e3 * span / args.requests, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded G500 R-MAT and Zipf)",
+        "config": {"workload": f"{args.requests} requests, Poisson {args.rate}/s, pool of {len(pool)} distinct",
+                   "slots": args.slots, "budget_bytes": 60e9, "products": flop},
+        "latency_s": {"p50": round(float(np.percentile(lat, 50)), 4), "p99": round(float(np.percentile(lat, 99)), 4),
+                      "max": round(float(lat.max()), 4)},
+        "gflops": round(2.0 * flop / span / 1e9, 3),
+        "server": st, "chunked_requests": int(st["chunked"]), "rejected": int(st["failed"]),
+        "alone_service_s": {"p50": round(float(np.percentile([v[3] for v in solo.values()], 50)), 4),
+                            "max": round(float(max(v[3] for v in solo.values())), 4)},
+        "results_equal_alone": True,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", default="product", choices=["product", "batch"],
-                    help="product: one large SpGEMM (the headline); batch: the uneven batch of jobs")
+    ap.add_argument("--mode", default="product", choices=["product", "batch", "serve"],
+                    help="product: one large SpGEMM (the headline); batch: the uneven batch of jobs; "
+                         "serve: the Poisson request stream")
+    ap.add_argument("--requests", type=int, default=200, help="serve mode: requests in the stream")
+    ap.add_argument("--rate", type=float, default=5.0, help="serve mode: Poisson arrival rate, requests/s")
+    ap.add_argument("--slots", type=int, default=4, help="serve mode: requests in flight at once")
+    ap.add_argument("--pool", type=int, default=32, help="serve mode: distinct requests the stream draws from")
     ap.add_argument("--jobs", type=int, default=512, help="batch mode: number of jobs")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -305,6 +406,8 @@ def main():
         return run_reference_arm(args, rank, world)
     if args.mode == "batch":
         return run_batch_mode(args) if rank == 0 else 0
+    if args.mode == "serve":
+        return run_serve_mode(args) if rank == 0 else 0
 
     import torch
     import casgemm

@@ -80,6 +80,28 @@ class CasBatchStats(ctypes.Structure):
 BATCH_MODES = {"waves": 0, "per_call": 1}
 
 
+class CasServerOpts(ctypes.Structure):
+    _fields_ = [
+        ("slots", ctypes.c_int32), ("accum", ctypes.c_int32), ("mem_budget", ctypes.c_double),
+        ("keep_output", ctypes.c_int32), ("dry_run", ctypes.c_int32), ("dry_run_ns_per_byte", ctypes.c_double),
+    ]
+
+
+class CasResult(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32), ("chunks", ctypes.c_int32), ("flop", ctypes.c_int64), ("nnz_c", ctypes.c_int64),
+        ("digest", ctypes.c_uint64), ("bound", ctypes.c_double), ("t_submit", ctypes.c_double),
+        ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double), ("C", CasCsr),
+    ]
+
+
+class CasServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+        ("chunked", ctypes.c_int64), ("max_inflight", ctypes.c_int32), ("max_inflight_bytes", ctypes.c_double),
+    ]
+
+
 class CasError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"{STATUS.get(status, status)}: {msg}")
@@ -111,6 +133,13 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "cas_csr_free": (I32, [P, ctypes.POINTER(CasCsr)]),
         "cas_csr_digest": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(ctypes.c_uint64), P]),
         "cas_batch_run": (I32, [P, I32, ctypes.POINTER(CasJob), I64, I32, D, ctypes.POINTER(CasBatchStats)]),
+        "cas_serve_create": (I32, [ctypes.c_int, ctypes.POINTER(CasServerOpts), ctypes.POINTER(P)]),
+        "cas_serve_submit": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), ctypes.POINTER(I64)]),
+        "cas_serve_poll": (I32, [P, I64, ctypes.POINTER(CasResult)]),
+        "cas_serve_wait": (I32, [P, I64, D, ctypes.POINTER(CasResult)]),
+        "cas_serve_stats": (I32, [P, ctypes.POINTER(CasServerStats)]),
+        "cas_serve_clock": (D, [P]),
+        "cas_serve_destroy": (None, [P]),
         "cas_flp_populate": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), P]),
         "cas_scan": (I32, [P, P, P, I64]),
         "cas_hash_symb": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), P, P]),
@@ -323,6 +352,86 @@ class Context:
         if rc != 0:
             raise CasError(rc, self.lib.cas_last_error(self.h).decode())
         return out, st.as_dict()
+
+
+class Server:
+    """A request loop with continuous batching (cas_serve_*): submit returns at
+    once; requests are admitted in order as slots and device memory free up,
+    and run concurrently."""
+
+    def __init__(self, device: int = 0, slots: int = 4, mem_budget: float = 60e9, accum: str = "hybacc",
+                 keep_output: bool = False, dry_run: bool = False, dry_run_ns_per_byte: float = 0.0):
+        self.lib = load()
+        opts = CasServerOpts(slots, ACCUM[accum], float(mem_budget), int(keep_output), int(dry_run),
+                             float(dry_run_ns_per_byte))
+        h = ctypes.c_void_p()
+        st = self.lib.cas_serve_create(device, ctypes.byref(opts), ctypes.byref(h))
+        if st != 0:
+            raise CasError(st, "cas_serve_create failed")
+        self.h = h
+        self._inputs = {}
+
+    def submit(self, A: Csr, B: Csr) -> int:
+        ca, cb = A.as_cas(), B.as_cas()
+        rid = ctypes.c_int64()
+        st = self.lib.cas_serve_submit(self.h, ctypes.byref(ca), ctypes.byref(cb), ctypes.byref(rid))
+        if st != 0:
+            raise CasError(st, "cas_serve_submit rejected the request")
+        self._inputs[rid.value] = (A, B, ca, cb)  # the server reads these arrays until the request completes
+        return rid.value
+
+    def _result(self, rid, r: CasResult) -> dict:
+        self._inputs.pop(rid, None)
+        out = {"status": r.status, "chunks": r.chunks, "flop": r.flop, "nnz_c": r.nnz_c, "digest": int(r.digest),
+               "bound": r.bound, "t_submit": r.t_submit, "t_admit": r.t_admit, "t_done": r.t_done}
+        if r.C.owned:
+            c = r.C
+            rp = np.ctypeslib.as_array(ctypes.cast(c.row_ptrs, ctypes.POINTER(ctypes.c_int64)), (c.num_row + 1,)).copy()
+            vt = ctypes.c_double if c.val_type == VAL_F64 else ctypes.c_int64
+            cols = (np.ctypeslib.as_array(ctypes.cast(c.cols, ctypes.POINTER(ctypes.c_int32)), (c.num_nnz,)).copy()
+                    if c.num_nnz else np.zeros(0, np.int32))
+            vals = (np.ctypeslib.as_array(ctypes.cast(c.rats, ctypes.POINTER(vt)), (c.num_nnz,)).copy()
+                    if c.num_nnz else np.zeros(0, np.float64 if c.val_type == VAL_F64 else np.int64))
+            out["C"] = Csr(c.num_row, c.num_col, rp, cols, vals)
+            self.lib.cas_csr_free(None, ctypes.byref(r.C))
+        return out
+
+    def poll(self, rid: int):
+        r = CasResult()
+        st = self.lib.cas_serve_poll(self.h, rid, ctypes.byref(r))
+        if st == 5:
+            return None
+        if st != 0:
+            raise CasError(st, f"unknown request {rid}")
+        return self._result(rid, r)
+
+    def wait(self, rid: int, timeout: float = -1.0):
+        r = CasResult()
+        st = self.lib.cas_serve_wait(self.h, rid, float(timeout), ctypes.byref(r))
+        if st == 5:
+            return None
+        if st != 0:
+            raise CasError(st, f"unknown request {rid}")
+        return self._result(rid, r)
+
+    def stats(self) -> dict:
+        s = CasServerStats()
+        self.lib.cas_serve_stats(self.h, ctypes.byref(s))
+        return {n: getattr(s, n) for n, _ in s._fields_}
+
+    def clock(self) -> float:
+        return self.lib.cas_serve_clock(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cas_serve_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 # ---------------------------------------------------------------- data layer

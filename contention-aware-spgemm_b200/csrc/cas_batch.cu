@@ -28,7 +28,8 @@ __device__ __forceinline__ uint64_t val_bits(long long v) { return (uint64_t)v; 
 
 // One warp per row of a product's rows [0, m) (global row g0 + r of the
 // batch): the row digest, folded into its job's digest.  job_of == nullptr
-// means a single job 0 with no shifts.
+// means a single job 0 with no shifts, whose rows [0, m) are its rows
+// [g0, g0 + m) (a row chunk of a larger product).
 template <typename OT>
 __global__ void __launch_bounds__(256)
 k_row_digest(int64_t m, int64_t g0, const int64_t* __restrict__ rp, const int32_t* __restrict__ col,
@@ -40,7 +41,7 @@ k_row_digest(int64_t m, int64_t g0, const int64_t* __restrict__ rp, const int32_
   for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
     const int64_t g = g0 + r;
     const int j = job_of ? job_of[g] : 0;
-    const int64_t rloc = job_of ? g - row_base[j] : r;
+    const int64_t rloc = job_of ? g - row_base[j] : g;
     const uint64_t cb = job_of ? (uint64_t)col_base[j] : 0ull;
     const int64_t s = rp[r], e = rp[r + 1];
     uint64_t h = 0;

@@ -218,6 +218,65 @@ typedef struct {
 cas_status cas_batch_run(cas_ctx *ctx, cas_accum accum, cas_job *jobs, int64_t n, cas_batch_mode mode,
 	double wave_budget, cas_batch_stats *stats);
 
+/* ---- serving: a request loop with continuous batching --------------------
+ *
+ * No counterpart in the reference.  A server owns `slots` worker threads,
+ * each with its own context and streams on one device.  cas_serve_submit
+ * queues a request and returns at once.  Requests are admitted in arrival
+ * order, each when a slot is free and its device-memory bound fits the
+ * budget beside the requests already running:
+ *   bound = 12 * sum over rows of min(row products, B.num_col) + 40 * (m + 1)
+ *           + the device copies of A and B
+ * (C's entries and row pointers, A's row pointers and the pipeline's per-row
+ * scratch), computed at submission from the row products.  Admitted requests
+ * run concurrently on the device, and later arrivals join as slots and
+ * memory free up.  A request whose bound exceeds the whole budget runs in row
+ * chunks that each fit.  Inputs are host CSRs (col_bytes 4); the server
+ * reads a request's A and B until it completes, so the caller keeps those
+ * arrays alive until then.  Times are seconds on the server's monotonic
+ * clock (cas_serve_clock). */
+typedef struct cas_server cas_server;
+
+typedef struct {
+	int32_t slots;              /* requests in flight at once (default 4) */
+	int32_t accum;              /* cas_accum (default CAS_ACC_HASH = 0; set CAS_ACC_HYBACC explicitly) */
+	double mem_budget;          /* device bytes for admitted requests (<= 0: 60e9) */
+	int32_t keep_output;        /* 1: C returned in host memory (cas_result.C) */
+	int32_t dry_run;            /* 1: no device work; a request takes dry_run_ns_per_byte * bound ns
+	                               (tests of the scheduler on machines without a GPU) */
+	double dry_run_ns_per_byte;
+} cas_server_opts;
+
+typedef struct {
+	int32_t status;             /* cas_status of the request */
+	int32_t chunks;             /* row chunks it ran in (1 unless its bound exceeded the budget) */
+	int64_t flop;
+	int64_t nnz_c;
+	uint64_t digest;            /* cas_csr_digest of C */
+	double bound;               /* device bytes reserved while it ran */
+	double t_submit, t_admit, t_done;
+	cas_csr C;                  /* keep_output: host C, freed with cas_csr_free(NULL, &C) */
+} cas_result;
+
+typedef struct {
+	int64_t submitted, completed, failed, chunked;
+	int32_t max_inflight;       /* most requests running at once */
+	double max_inflight_bytes;  /* largest sum of reserved bounds at once */
+} cas_server_stats;
+
+cas_status cas_serve_create(int device, const cas_server_opts *opts, cas_server **out);
+/* Queues C = A * B; *id names the request. */
+cas_status cas_serve_submit(cas_server *srv, const cas_csr *A, const cas_csr *B, int64_t *id);
+/* CAS_OK with *out filled once request `id` completed (the id is then
+ * released); CAS_ERR_TIMEOUT while it has not.  cas_serve_wait blocks up to
+ * timeout_s seconds (< 0: without limit). */
+cas_status cas_serve_poll(cas_server *srv, int64_t id, cas_result *out);
+cas_status cas_serve_wait(cas_server *srv, int64_t id, double timeout_s, cas_result *out);
+cas_status cas_serve_stats(cas_server *srv, cas_server_stats *out);
+double cas_serve_clock(const cas_server *srv);
+/* Completes every queued request, then stops the workers. */
+void cas_serve_destroy(cas_server *srv);
+
 /* ---- scan that allocates nothing ---------------------------------------- */
 
 /* The exclusive scan of cas_scan (d_out[0] = 0, d_out[i+1] = d_out[i] +
