@@ -13,8 +13,14 @@
 // call, each to size the next phase (bin counts, nnz(C)).
 #include <cuda_runtime.h>
 
+#include <immintrin.h>
+#include <sys/mman.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <mutex>
+#include <thread>
+#include <unordered_map>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -63,8 +69,13 @@ struct cas_ctx {
   unsigned long long* d_counts = nullptr;
   unsigned long long* h_counts = nullptr;  // pinned mirror
   cas::DevStatus* h_status = nullptr;      // pinned mirror
-  void* h_stage[2] = {};                   // pinned staging for large host copies
-  cudaEvent_t ev_stage[2] = {};
+  void* h_stage[3] = {};                   // pinned staging for large host copies
+  cudaEvent_t ev_stage[3] = {};
+  // host blocks of returned C arrays: capacity of every live block this
+  // context allocated, and the released ones kept for reuse
+  std::unordered_map<void*, size_t> host_blocks;
+  std::vector<std::pair<void*, size_t>> host_free;
+  size_t host_free_bytes = 0;
 };
 
 namespace {
@@ -240,35 +251,145 @@ cas_status dev_alloc(cas_ctx* ctx, void** p, size_t bytes) {
   return CAS_OK;
 }
 
-// Device -> pageable host copy through two pinned staging buffers: the copy
-// of chunk i runs on the DMA engine while host threads move chunk i-1 out of
-// staging (and fault in the destination pages in parallel).
-cas_status d2h_staged(cas_ctx* ctx, void* dst, const void* src, size_t bytes) {
+// Host memory for C: 2 MiB-aligned and marked for transparent huge pages,
+// so first touch faults once per 2 MiB instead of once per 4 KiB (the copy
+// into fresh 4 KiB pages runs at a third of the DMA rate).  Freed with free().
+void* host_alloc_huge(size_t bytes) {
+  constexpr size_t kHuge = size_t(2) << 20;
+  const size_t len = (bytes + kHuge - 1) / kHuge * kHuge;
+  void* p = nullptr;
+  if (posix_memalign(&p, kHuge, len ? len : kHuge) != 0) return nullptr;
+  madvise(p, len ? len : kHuge, MADV_HUGEPAGE);  // advisory: ignored where THP is off
+  return p;
+}
+
+// Host blocks for returned C arrays.  A block released through cas_csr_free
+// stays with the context, its pages resident, and serves the next output of
+// up to its size (but not one under half of it); a context keeps at most
+// kHostCacheShare of physical memory this way and frees the rest.  Fresh
+// pages cost a fault per 2 MiB during the copy; resident ones let the copy
+// run at the DMA rate.
+constexpr double kHostCacheShare = 0.6;
+
+void* host_take(cas_ctx* ctx, size_t bytes) {
+  size_t best = SIZE_MAX;
+  size_t bi = 0;
+  for (size_t i = 0; i < ctx->host_free.size(); ++i) {
+    const size_t cap = ctx->host_free[i].second;
+    if (cap >= bytes && cap / 2 <= bytes && cap < best) {
+      best = cap;
+      bi = i;
+    }
+  }
+  if (best != SIZE_MAX) {
+    void* p = ctx->host_free[bi].first;
+    ctx->host_free_bytes -= best;
+    ctx->host_free.erase(ctx->host_free.begin() + (std::ptrdiff_t)bi);
+    return p;
+  }
+  void* p = host_alloc_huge(bytes);
+  if (p) ctx->host_blocks[p] = bytes;
+  return p;
+}
+
+void host_give(cas_ctx* ctx, void* p) {
+  if (!p) return;
+  auto it = ctx ? ctx->host_blocks.find(p) : decltype(ctx->host_blocks)::iterator();
+  if (!ctx || it == ctx->host_blocks.end()) {
+    free(p);
+    return;
+  }
+  static const double phys = (double)sysconf(_SC_PHYS_PAGES) * (double)sysconf(_SC_PAGESIZE);
+  if ((double)(ctx->host_free_bytes + it->second) > kHostCacheShare * phys) {
+    ctx->host_blocks.erase(it);
+    free(p);
+    return;
+  }
+  ctx->host_free.emplace_back(p, it->second);
+  ctx->host_free_bytes += it->second;
+}
+
+// Copies out of a staging buffer with non-temporal stores: the destination
+// lines are written without being read first, which is a third less memory
+// traffic than a plain copy of data that is not reused soon.  Falls back to
+// memcpy for a misaligned destination and for the tail.
+__attribute__((target("avx2"))) void stream_copy(char* d, const char* s, size_t n) {
+  if ((reinterpret_cast<uintptr_t>(d) & 31) || (reinterpret_cast<uintptr_t>(s) & 31)) {
+    memcpy(d, s, n);
+    return;
+  }
+  const size_t v = n / 128;
+  for (size_t i = 0; i < v; ++i) {
+    const __m256i* src = reinterpret_cast<const __m256i*>(s) + 4 * i;
+    __m256i* dst = reinterpret_cast<__m256i*>(d) + 4 * i;
+    const __m256i a = _mm256_load_si256(src), b = _mm256_load_si256(src + 1);
+    const __m256i c = _mm256_load_si256(src + 2), e = _mm256_load_si256(src + 3);
+    _mm256_stream_si256(dst, a);
+    _mm256_stream_si256(dst + 1, b);
+    _mm256_stream_si256(dst + 2, c);
+    _mm256_stream_si256(dst + 3, e);
+  }
+  memcpy(d + v * 128, s + v * 128, n - v * 128);
+  _mm_sfence();
+}
+
+// int32 -> int64 widening copy with non-temporal stores (n int32 values).
+__attribute__((target("avx2"))) void stream_widen(int64_t* d, const int32_t* s, size_t n) {
+  size_t i = 0;
+  if (!(reinterpret_cast<uintptr_t>(d) & 31) && !(reinterpret_cast<uintptr_t>(s) & 15)) {
+    for (; i + 8 <= n; i += 8) {
+      const __m128i lo = _mm_load_si128(reinterpret_cast<const __m128i*>(s + i));
+      const __m128i hi = _mm_load_si128(reinterpret_cast<const __m128i*>(s + i + 4));
+      _mm256_stream_si256(reinterpret_cast<__m256i*>(d + i), _mm256_cvtepi32_epi64(lo));
+      _mm256_stream_si256(reinterpret_cast<__m256i*>(d + i + 4), _mm256_cvtepi32_epi64(hi));
+    }
+    _mm_sfence();
+  }
+  for (; i < n; ++i) d[i] = s[i];
+}
+
+// Device -> pageable host copy through pinned staging buffers: the DMA of
+// chunk i runs while host threads move chunk i-1 out of staging.  With
+// `widen`, the source holds int32 and the destination int64 (bytes counts
+// the source).
+constexpr int kStageBufs = 3;
+cas_status d2h_staged(cas_ctx* ctx, void* dst, const void* src, size_t bytes, bool widen = false) {
   if (bytes == 0) return CAS_OK;
   if (!ctx->h_stage[0]) {
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kStageBufs; ++i) {
       CAS_CUDA(ctx, cudaMallocHost(&ctx->h_stage[i], kStageBytes));
       CAS_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_stage[i], cudaEventDisableTiming));
     }
   }
   const size_t nchunk = (bytes + kStageBytes - 1) / kStageBytes;
-  for (size_t i = 0; i <= nchunk; ++i) {
-    if (i < nchunk) {
-      const size_t off = i * kStageBytes, len = std::min(kStageBytes, bytes - off);
-      CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage[i & 1], static_cast<const char*>(src) + off, len,
-                                    cudaMemcpyDeviceToHost, ctx->stream));
-      CAS_CUDA(ctx, cudaEventRecord(ctx->ev_stage[i & 1], ctx->stream));
-    }
-    if (i > 0) {
-      const size_t j = i - 1, off = j * kStageBytes, len = std::min(kStageBytes, bytes - off);
-      CAS_CUDA(ctx, cudaEventSynchronize(ctx->ev_stage[j & 1]));
+  auto issue = [&](size_t i) -> cas_status {
+    const size_t off = i * kStageBytes, len = std::min(kStageBytes, bytes - off);
+    CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage[i % kStageBufs], static_cast<const char*>(src) + off, len,
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    CAS_CUDA(ctx, cudaEventRecord(ctx->ev_stage[i % kStageBufs], ctx->stream));
+    return CAS_OK;
+  };
+  for (size_t i = 0; i < std::min<size_t>(kStageBufs - 1, nchunk); ++i) CAS_TRY(issue(i));
+  for (size_t j = 0; j < nchunk; ++j) {
+    if (j + kStageBufs - 1 < nchunk) CAS_TRY(issue(j + kStageBufs - 1));
+    const size_t off = j * kStageBytes, len = std::min(kStageBytes, bytes - off);
+    CAS_CUDA(ctx, cudaEventSynchronize(ctx->ev_stage[j % kStageBufs]));
+    const char* s = static_cast<const char*>(ctx->h_stage[j % kStageBufs]);
+    const int64_t pieces = (int64_t)((len + (1 << 20) - 1) >> 20);
+    if (widen) {
+      const int32_t* s32 = reinterpret_cast<const int32_t*>(s);
+      int64_t* d64 = static_cast<int64_t*>(dst) + off / 4;
+#pragma omp parallel for schedule(static)
+      for (int64_t p = 0; p < pieces; ++p) {
+        const size_t o = (size_t)p << 18, e = std::min(o + ((size_t)1 << 18), len / 4);
+        stream_widen(d64 + o, s32 + o, e - o);
+      }
+    } else {
       char* d = static_cast<char*>(dst) + off;
-      const char* s = static_cast<const char*>(ctx->h_stage[j & 1]);
-      const int64_t pieces = (int64_t)((len + (1 << 20) - 1) >> 20);
 #pragma omp parallel for schedule(static)
       for (int64_t p = 0; p < pieces; ++p) {
         const size_t o = (size_t)p << 20;
-        memcpy(d + o, s + o, std::min((size_t)1 << 20, len - o));
+        stream_copy(d + o, s + o, std::min((size_t)1 << 20, len - o));
       }
     }
   }
@@ -672,18 +793,45 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
   void* cval = nullptr;
   CAS_TRY(dev_alloc(ctx, (void**)&ccol, sizeof(int32_t) * nnz));
   CAS_TRY(dev_alloc(ctx, &cval, vbytes * nnz));
-  CAS_TRY(numc_bins(ctx, c, crp, mode_of(accum)));
+  // host C
+  int64_t* h_rp = nullptr;
+  void *h_col = nullptr, *h_val = nullptr;
+  auto free_host = [&] {
+    host_give(ctx, h_rp);
+    host_give(ctx, h_col);
+    host_give(ctx, h_val);
+  };
+  if (!c_on_device) {
+    h_rp = static_cast<int64_t*>(host_take(ctx, sizeof(int64_t) * (c.m + 1)));
+    h_col = host_take(ctx, (size_t)c_col_bytes * (nnz > 0 ? nnz : 1));
+    h_val = host_take(ctx, vbytes * (nnz > 0 ? nnz : 1));
+    if (!h_rp || !h_col || !h_val) {
+      free_host();
+      return set_err(ctx, CAS_ERR_OOM, "host allocation of C failed");
+    }
+  }
+  {
+    cas_status st = numc_bins(ctx, c, crp, mode_of(accum));
+    if (st != CAS_OK) { free_host(); return st; }
+  }
   CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[3], ctx->stream));
   // NUMC
-  if (c.vt == CAS_VAL_F64) CAS_TRY(launch_numc_bins<double>(ctx, c, crp, ccol, cval));
-  else CAS_TRY(launch_numc_bins<int32_t>(ctx, c, crp, ccol, cval));
-  CAS_TRY(scratch_free(ctx, c));
-  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[4], ctx->stream));
-  CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotOvf, ctx->d_counts + kSlotOvf, sizeof(unsigned long long),
-                                cudaMemcpyDeviceToHost, ctx->stream));
-  CAS_TRY(check_status(ctx));
-  CAS_TRY(free_owned(ctx, c.A));
-  CAS_TRY(free_owned(ctx, c.B));
+  cas_status nst = [&]() -> cas_status {
+    if (c.vt == CAS_VAL_F64) CAS_TRY(launch_numc_bins<double>(ctx, c, crp, ccol, cval));
+    else CAS_TRY(launch_numc_bins<int32_t>(ctx, c, crp, ccol, cval));
+    CAS_TRY(scratch_free(ctx, c));
+    CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[4], ctx->stream));
+    CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotOvf, ctx->d_counts + kSlotOvf, sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    CAS_TRY(check_status(ctx));
+    CAS_TRY(free_owned(ctx, c.A));
+    CAS_TRY(free_owned(ctx, c.B));
+    return CAS_OK;
+  }();
+  if (nst != CAS_OK) {
+    free_host();
+    return nst;
+  }
 
   C->num_row = c.m;
   C->num_col = c.ncol;
@@ -697,28 +845,15 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
     C->cols = ccol;
     C->rats = cval;
   } else {
+    C->owned = 2;
     C->on_device = 0;
     C->col_bytes = c_col_bytes;
-    C->row_ptrs = static_cast<int64_t*>(malloc(sizeof(int64_t) * (c.m + 1)));
-    C->cols = malloc((size_t)c_col_bytes * (nnz > 0 ? nnz : 1));
-    C->rats = malloc(vbytes * (nnz > 0 ? nnz : 1));
-    if (!C->row_ptrs || !C->cols || !C->rats) {
-      free(C->row_ptrs); free(C->cols); free(C->rats);
-      memset(C, 0, sizeof(*C));
-      return set_err(ctx, CAS_ERR_OOM, "host allocation of C failed");
-    }
+    C->row_ptrs = h_rp;
+    C->cols = h_col;
+    C->rats = h_val;
     CAS_TRY(d2h_staged(ctx, C->row_ptrs, crp, sizeof(int64_t) * (c.m + 1)));
     CAS_TRY(d2h_staged(ctx, C->rats, cval, vbytes * nnz));
-    if (c_col_bytes == 4) {
-      CAS_TRY(d2h_staged(ctx, C->cols, ccol, sizeof(int32_t) * nnz));
-    } else {
-      // widen into the upper half-free int64 buffer: copy int32 into its
-      // first half, then widen from the back so nothing is overwritten early
-      CAS_TRY(d2h_staged(ctx, C->cols, ccol, sizeof(int32_t) * nnz));
-      const int32_t* c32 = static_cast<const int32_t*>(C->cols);
-      int64_t* c64 = static_cast<int64_t*>(C->cols);
-      for (int64_t i = nnz - 1; i >= 0; --i) c64[i] = c32[i];
-    }
+    CAS_TRY(d2h_staged(ctx, C->cols, ccol, sizeof(int32_t) * nnz, c_col_bytes == 8));
     d2h += sizeof(int64_t) * (double)(c.m + 1) + (vbytes + c_col_bytes) * (double)nnz;
     CAS_CUDA(ctx, cudaFreeAsync(crp, ctx->stream));
     CAS_CUDA(ctx, cudaFreeAsync(ccol, ctx->stream));
@@ -843,10 +978,11 @@ void cas_destroy(cas_ctx* ctx) {
   if (ctx->d_counts) cudaFree(ctx->d_counts);
   if (ctx->h_counts) cudaFreeHost(ctx->h_counts);
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < kStageBufs; ++i) {
     if (ctx->h_stage[i]) cudaFreeHost(ctx->h_stage[i]);
     if (ctx->ev_stage[i]) cudaEventDestroy(ctx->ev_stage[i]);
   }
+  for (auto& b : ctx->host_free) free(b.first);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
 }
@@ -903,9 +1039,10 @@ cas_status cas_csr_free(cas_ctx* ctx, cas_csr* C) {
         cudaFree(C->rats);
       }
     } else {
-      free(C->row_ptrs);
-      free(C->cols);
-      free(C->rats);
+      cas_ctx* owner = C->owned == 2 ? ctx : nullptr;  // 2: blocks of this context's host cache
+      host_give(owner, C->row_ptrs);
+      host_give(owner, C->cols);
+      host_give(owner, C->rats);
     }
   }
   memset(C, 0, sizeof(*C));

@@ -60,7 +60,8 @@ typedef struct {
 	int32_t col_bytes;   /* 4 or 8; device matrices use 4 */
 	int32_t val_type;    /* cas_valtype */
 	int32_t on_device;   /* 1: pointers are device memory of the context's device */
-	int32_t owned;       /* set by the library when it allocated the arrays; see cas_csr_free */
+	int32_t owned;       /* set by the library when it allocated the arrays (2: host arrays from the
+	                        context's block cache); see cas_csr_free */
 } cas_csr;
 
 /* Phase times in seconds, the reference's runtime_t (src/mm/mm_utils.h:48-54);
@@ -158,7 +159,12 @@ cas_status cas_hybacc_numc(cas_ctx *ctx, const cas_csr *A, const cas_csr *B, con
 cas_status cas_spgemm(cas_ctx *ctx, cas_accum accum, const cas_csr *A, const cas_csr *B, cas_csr *C,
 	cas_runtime *rt);
 
-/* Frees arrays the library allocated (owned != 0) and zeroes the struct. */
+/* Frees arrays the library allocated (owned != 0) and zeroes the struct.
+ * Host arrays of a C from cas_spgemm (owned 2) go back to the context that
+ * made them, which keeps up to 60% of physical memory of such blocks, pages
+ * resident, for later outputs (so repeated products into host memory skip
+ * the page faults); they are released at cas_destroy.  Passing another
+ * context or NULL frees them at once. */
 cas_status cas_csr_free(cas_ctx *ctx, cas_csr *C);
 
 /* ---- digests of a product ------------------------------------------------
