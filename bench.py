@@ -497,6 +497,9 @@ def main():
             bin_ms[k] = bin_ms.get(k, 0.0) + v / n_prof
             bin_bytes[k] = bin_bytes.get(k, 0.0) + s["numc_bin_bytes"][k] / n_prof
         ovf_rows, ovf_ms = s["esc_overflow_rows"], ovf_ms + s["esc_overflow_ms"] / n_prof
+        if s["fused_rows"]:
+            bin_ms["fused"] = bin_ms.get("fused", 0.0) + s["fused_ms"] / n_prof
+            bin_bytes["fused"] = bin_bytes.get("fused", 0.0) + s["fused_bytes"] / n_prof
     ctx.set_profiling(False)
 
     # roofline of the dominant kernel (the numeric bin with the most device time)
@@ -507,8 +510,12 @@ def main():
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9 if dom_ms > 0 else 0.0
     kernel_name = {"tiny": "k_numc_tiny<256>", "hash256": "k_numc_hash<256,9>", "hash1k": "k_numc_hash<256,11>",
                    "hash4k": "k_numc_hash<512,13>", "dense": "k_numc_dense<1024>"}.get(dom)
+    if dom == "fused":
+        kernel_name = "k_numc_esc_msd<256,4800,11,fused>"
     if kernel_name is None and dom.startswith("esc"):
-        kernel_name = f"k_numc_esc_msd<256,{int(dom[3:-1]) * 1024}>"
+        kernel_name = "k_numc_esc_msd<256,%s>" % {"esc1k": "1024,9", "esc2k": "2048,9", "esc3k": "3072,10",
+                                                   "esc4k": "4096,10", "esc5k": "4800,11", "esc6k": "6144,11",
+                                                   "esc8k": "8192,11"}[dom]
     alg_bytes_total = 12.0 * (A.nnz if world == 1 else As.nnz) + 12.0 * P_local + 12.0 * nnz_local + 16.0 * (As.num_row + 1)
     pipe_frac = alg_bytes_total / (ms_step * 1e-3) / (peak * 1e9)
 

@@ -55,6 +55,8 @@ class CasStats(ctypes.Structure):
         ("symb_bin_ms", ctypes.c_double * 9), ("numc_bin_ms", ctypes.c_double * 13),
         ("numc_bin_bytes", ctypes.c_double * 13), ("numc_bin_flop", ctypes.c_int64 * 13),
         ("esc_overflow_rows", ctypes.c_int64), ("esc_overflow_ms", ctypes.c_double),
+        ("fused_rows", ctypes.c_int64), ("fused_flop", ctypes.c_int64), ("fused_bytes", ctypes.c_double),
+        ("fused_ms", ctypes.c_double),
     ]
 
 
@@ -127,6 +129,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "cas_set_acc_thres": (I32, [P, D]),
         "cas_last_error": (ctypes.c_char_p, [P]),
         "cas_set_profiling": (I32, [P, ctypes.c_int]),
+        "cas_set_fusion": (I32, [P, ctypes.c_int]),
         "cas_get_stats": (I32, [P, ctypes.POINTER(CasStats)]),
         "cas_spgemm": (I32, [P, I32, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr),
                              ctypes.POINTER(CasRuntime)]),
@@ -253,6 +256,9 @@ class Context:
     def set_acc_thres(self, thres: float):
         self._check(self.lib.cas_set_acc_thres(self.h, float(thres)))
 
+    def set_fusion(self, on: bool):
+        self._check(self.lib.cas_set_fusion(self.h, int(bool(on))))
+
     def set_profiling(self, on: bool):
         self._check(self.lib.cas_set_profiling(self.h, int(bool(on))))
 
@@ -272,6 +278,8 @@ class Context:
             "numc_bin_bytes": dict(zip(NUMC_BINS, list(s.numc_bin_bytes))),
             "numc_bin_flop": dict(zip(NUMC_BINS, list(s.numc_bin_flop))),
             "esc_overflow_rows": s.esc_overflow_rows, "esc_overflow_ms": s.esc_overflow_ms,
+            "fused_rows": s.fused_rows, "fused_flop": s.fused_flop, "fused_bytes": s.fused_bytes,
+            "fused_ms": s.fused_ms,
         }
 
     def spgemm(self, A, B, accum: str = "hybacc", col_bytes: int = 4) -> Result:

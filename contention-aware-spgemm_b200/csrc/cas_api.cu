@@ -44,6 +44,7 @@ constexpr int kSlotNnz = 44;     // [44]    nnz(C) from the scan
 constexpr int kSlotCheck = 48;   // [48, 52) input check flags
 constexpr int kSlotBinSums = 64; // [64, 103) per numeric bin: products, nnz(C), nnz(A)
 constexpr int kSlotOvf = 110;    // [110]   rows handed to the radix-sort ESC kernel
+constexpr int kSlotFused = 112;  // [112, 116) fused rows: count, products, output bound, nnz(A); [116] ticket
 constexpr size_t kStageBytes = size_t(64) << 20;  // pinned staging chunk for host copies
 
 }  // namespace
@@ -61,7 +62,9 @@ struct cas_ctx {
   cudaEvent_t ev_numc[2][cas::kNumcBins] = {};
   cudaEvent_t ev_ovf[2] = {};
   bool profile = false;
+  bool fuse = true;                        // fused ESC rows (no symbolic pass) in cas_spgemm
   double acc_thres = 2.0;
+  cudaEvent_t ev_fused[2] = {};
   std::string err;
   cas_stats stats{};
   int64_t launches = 0;
@@ -200,6 +203,8 @@ cas_status setup_numc_kernels(cas_ctx* ctx) {
   CAS_TRY(allow_smem(ctx, k_numc_esc_msd<256, CAP, NBB, VIn>, smem_numc_esc_msd<CAP, NBB, VIn>()));
   CAS_ESC_SHAPES(CAS_SETUP_ESC)
 #undef CAS_SETUP_ESC
+  CAS_TRY(allow_smem(ctx, k_numc_esc_msd<256, (int)kFusedHi, 11, VIn, true>,
+                     smem_numc_esc_msd<(int)kFusedHi, 11, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_esc_overflow<1024, 8192, VIn>, smem_numc_esc<1024, 8192, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_hash<256, 9, VIn>, smem_numc_hash<256, 9, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_hash<256, 11, VIn>, smem_numc_hash<256, 11, VIn>()));
@@ -498,6 +503,13 @@ struct Call {
   int64_t symb_count[cas::kSymbBins] = {};
   int64_t numc_count[cas::kNumcBins] = {};
   int64_t flop = 0, max_flp = 0;
+  // fused rows (cas_spgemm with ESC or hybrid accumulation)
+  int fuse = 0;
+  int64_t nf = 0, f_flop = 0, f_bound = 0, f_nnza = 0;
+  int32_t* frows = nullptr;
+  int64_t* fpos = nullptr;
+  unsigned long long* fstatus = nullptr;
+  bool ovf_preset = false;
 };
 
 cas_status fork(cas_ctx* ctx) {
@@ -524,12 +536,15 @@ cas_status scratch_alloc(cas_ctx* ctx, Call& c) {
 }
 
 cas_status scratch_free(cas_ctx* ctx, Call& c) {
-  void* ps[] = {c.row_flp, c.row_nz, c.rows, c.ovf, c.partial};
+  void* ps[] = {c.row_flp, c.row_nz, c.rows, c.ovf, c.partial, c.frows, c.fpos, c.fstatus};
   for (void* p : ps)
     if (p) CAS_CUDA(ctx, cudaFreeAsync(p, ctx->stream));
   c.row_flp = c.row_nz = nullptr;
   c.rows = c.ovf = nullptr;
   c.partial = nullptr;
+  c.frows = nullptr;
+  c.fpos = nullptr;
+  c.fstatus = nullptr;
   return CAS_OK;
 }
 
@@ -566,7 +581,8 @@ cas_status phase_init(cas_ctx* ctx, Call& c, bool validate) {
   }
   if (c.m > 0) {
     k_flp<256><<<grid_for(c.m * 32, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
-        c.A.csr, c.B.csr, c.ncol, c.row_flp, ctx->d_counts + kSlotTotals, ctx->d_counts + kSlotSymb, ctx->d_status);
+        c.A.csr, c.B.csr, c.ncol, c.row_flp, ctx->d_counts + kSlotTotals, ctx->d_counts + kSlotSymb, ctx->d_status,
+        c.fuse, ctx->d_counts + kSlotFused);
     CAS_TRY(check_launch(ctx, "k_flp"));
   }
   CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, sizeof(unsigned long long) * kCountSlots,
@@ -581,6 +597,10 @@ cas_status phase_init(cas_ctx* ctx, Call& c, bool validate) {
   }
   c.flop = (int64_t)ctx->h_counts[kSlotTotals];
   c.max_flp = (int64_t)ctx->h_counts[kSlotTotals + 1];
+  c.nf = (int64_t)ctx->h_counts[kSlotFused];
+  c.f_flop = (int64_t)ctx->h_counts[kSlotFused + 1];
+  c.f_bound = (int64_t)ctx->h_counts[kSlotFused + 2];
+  c.f_nnza = (int64_t)ctx->h_counts[kSlotFused + 3];
   unsigned long long* cur = ctx->h_counts + kSlotCursor;
   unsigned long long off = 0;
   for (int b = 0; b < kSymbBins; ++b) {
@@ -592,9 +612,47 @@ cas_status phase_init(cas_ctx* ctx, Call& c, bool validate) {
     CAS_CUDA(ctx, cudaMemcpyAsync(ctx->d_counts + kSlotCursor, cur, sizeof(unsigned long long) * kSymbBins,
                                   cudaMemcpyHostToDevice, ctx->stream));
     k_bin_scatter_symb<<<grid_for(c.m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
-        c.m, c.row_flp, c.ncol, ctx->d_counts + kSlotCursor, c.rows);
+        c.m, c.row_flp, c.ncol, ctx->d_counts + kSlotCursor, c.rows, c.fuse);
     CAS_TRY(check_launch(ctx, "k_bin_scatter_symb"));
   }
+  if (c.nf > 0) {
+    // the fused rows in ascending order: marks (in row_nz, cleared before the
+    // symbolic kernels), their scan, the scatter
+    CAS_TRY(dev_alloc(ctx, (void**)&c.fpos, sizeof(int64_t) * (c.m + 1)));
+    CAS_TRY(dev_alloc(ctx, (void**)&c.frows, sizeof(int32_t) * c.nf));
+    CAS_TRY(dev_alloc(ctx, (void**)&c.fstatus, sizeof(unsigned long long) * c.nf));
+    const int g = grid_for(c.m, 256, ctx->sm_count * 8);
+    k_fused_mark<<<g, 256, 0, ctx->stream>>>(c.m, c.row_flp, c.fuse, c.row_nz);
+    CAS_TRY(check_launch(ctx, "k_fused_mark"));
+    CAS_TRY(launch_scan(ctx, c.fpos, c.row_nz, c.m + 1, c.partial, nullptr));
+    k_fused_scatter<<<g, 256, 0, ctx->stream>>>(c.m, c.row_flp, c.fuse, c.fpos, c.frows);
+    CAS_TRY(check_launch(ctx, "k_fused_scatter"));
+  }
+  return CAS_OK;
+}
+
+// ------------------------------------------------------------- FUSED ROWS
+// The fused ESC kernel over the fused rows, in row order: each writes its row
+// of C at known[r] (the scan of the other rows' counts) plus the counts of the
+// fused rows before it, and its count into row_nz.
+template <typename VIn>
+cas_status launch_fused(cas_ctx* ctx, Call& c, const int64_t* known, int32_t* ccol, void* cval, int64_t cap) {
+  using namespace cas;
+  using AT = typename Acc<VIn>::T;
+  if (c.nf == 0) return CAS_OK;
+  unsigned int* ovf_count = reinterpret_cast<unsigned int*>(ctx->d_counts + kSlotOvf);
+  CAS_CUDA(ctx, cudaMemsetAsync(ovf_count, 0, sizeof(unsigned int), ctx->stream));
+  c.ovf_preset = true;
+  CAS_CUDA(ctx, cudaMemsetAsync(c.fstatus, 0, sizeof(unsigned long long) * c.nf, ctx->stream));
+  CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + kSlotFused + 4, 0, sizeof(unsigned long long), ctx->stream));
+  Fused fu{c.frows, ctx->d_counts + kSlotFused + 4, c.fstatus, known, c.row_nz, cap};
+  if (ctx->profile) CAS_CUDA(ctx, cudaEventRecord(ctx->ev_fused[0], ctx->stream));
+  k_numc_esc_msd<256, (int)kFusedHi, 11, VIn, true>
+      <<<(unsigned)c.nf, 256, smem_numc_esc_msd<(int)kFusedHi, 11, VIn>(), ctx->stream>>>(
+          nullptr, c.A.csr, c.B.csr, c.b_sorted ? 1 : 0, nullptr, ccol, static_cast<AT*>(cval), c.ovf, ovf_count,
+          ctx->d_status, fu);
+  CAS_TRY(check_launch(ctx, "k_numc_esc_msd (fused)"));
+  if (ctx->profile) CAS_CUDA(ctx, cudaEventRecord(ctx->ev_fused[1], ctx->stream));
   return CAS_OK;
 }
 
@@ -684,9 +742,9 @@ cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* 
   const int order[] = {kNB_Dense, kNB_E8K, kNB_H4K, kNB_E6K, kNB_E5K, kNB_E4K, kNB_E3K, kNB_H1K,
                        kNB_E2K, kNB_E1K, kNB_H256, kNB_Tiny};
   unsigned int* ovf_count = reinterpret_cast<unsigned int*>(ctx->d_counts + kSlotOvf);
-  CAS_CUDA(ctx, cudaMemsetAsync(ovf_count, 0, sizeof(unsigned int), ctx->stream));
+  if (!c.ovf_preset) CAS_CUDA(ctx, cudaMemsetAsync(ovf_count, 0, sizeof(unsigned int), ctx->stream));
   CAS_TRY(fork(ctx));
-  int64_t esc_rows = 0;
+  int64_t esc_rows = c.nf;  // fused rows may have handed rows to the radix-sort kernel too
   int si = 0;
   for (int b : order) {
     const int64_t n = c.numc_count[b];
@@ -704,7 +762,7 @@ cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* 
       case bin:                                                                                         \
         esc_rows += n;                                                                                  \
         k_numc_esc_msd<256, CAP, NBB, VIn><<<(unsigned)n, 256, smem_numc_esc_msd<CAP, NBB, VIn>(), s>>>( \
-            rows, A, B, c.b_sorted ? 1 : 0, crp, ccol, cval, c.ovf, ovf_count, ctx->d_status);          \
+            rows, A, B, c.b_sorted ? 1 : 0, crp, ccol, cval, c.ovf, ovf_count, ctx->d_status, Fused{});  \
         break;
       CAS_ESC_SHAPES(CAS_ESC_CASE)
 #undef CAS_ESC_CASE
@@ -772,6 +830,7 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
   const int c_col_bytes = c_on_device ? 4 : (C->col_bytes == 8 ? 8 : 4);
   CAS_TRY(prepare(ctx, A, B, c, h2d));
   memset(C, 0, sizeof(*C));
+  c.fuse = ctx->fuse && accum != CAS_ACC_HASH ? 1 : 0;
   const size_t vbytes = 8;  // fp64 or int64 output
   CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[0], ctx->stream));
   // INIT
@@ -786,13 +845,17 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
   CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotNnz, ctx->d_counts + kSlotNnz, sizeof(unsigned long long),
                                 cudaMemcpyDeviceToHost, ctx->stream));
   CAS_TRY(check_status(ctx));
-  const int64_t nnz = (int64_t)ctx->h_counts[kSlotNnz];
+  // counts of the rows that had a symbolic pass; the fused rows add theirs
+  // in NUMC, within the bound min(products, columns) each
+  const int64_t nnz_known = (int64_t)ctx->h_counts[kSlotNnz];
+  const int64_t cap = nnz_known + (c.nf > 0 ? c.f_bound : 0);
+  int64_t nnz = nnz_known;
   CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[2], ctx->stream));
   // MGMT
   int32_t* ccol = nullptr;
   void* cval = nullptr;
-  CAS_TRY(dev_alloc(ctx, (void**)&ccol, sizeof(int32_t) * nnz));
-  CAS_TRY(dev_alloc(ctx, &cval, vbytes * nnz));
+  CAS_TRY(dev_alloc(ctx, (void**)&ccol, sizeof(int32_t) * cap));
+  CAS_TRY(dev_alloc(ctx, &cval, vbytes * cap));
   // host C
   int64_t* h_rp = nullptr;
   void *h_col = nullptr, *h_val = nullptr;
@@ -803,8 +866,8 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
   };
   if (!c_on_device) {
     h_rp = static_cast<int64_t*>(host_take(ctx, sizeof(int64_t) * (c.m + 1)));
-    h_col = host_take(ctx, (size_t)c_col_bytes * (nnz > 0 ? nnz : 1));
-    h_val = host_take(ctx, vbytes * (nnz > 0 ? nnz : 1));
+    h_col = host_take(ctx, (size_t)c_col_bytes * (cap > 0 ? cap : 1));
+    h_val = host_take(ctx, vbytes * (cap > 0 ? cap : 1));
     if (!h_rp || !h_col || !h_val) {
       free_host();
       return set_err(ctx, CAS_ERR_OOM, "host allocation of C failed");
@@ -817,13 +880,24 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
   CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[3], ctx->stream));
   // NUMC
   cas_status nst = [&]() -> cas_status {
+    if (c.nf > 0) {
+      // fused rows first (they place themselves after the known counts), then
+      // the scan of all counts, which the other kernels write by
+      if (c.vt == CAS_VAL_F64) CAS_TRY(launch_fused<double>(ctx, c, crp, ccol, cval, cap));
+      else CAS_TRY(launch_fused<int32_t>(ctx, c, crp, ccol, cval, cap));
+      CAS_TRY(launch_scan(ctx, crp, c.row_nz, c.m + 1, c.partial,
+                          reinterpret_cast<int64_t*>(ctx->d_counts + kSlotNnz)));
+    }
     if (c.vt == CAS_VAL_F64) CAS_TRY(launch_numc_bins<double>(ctx, c, crp, ccol, cval));
     else CAS_TRY(launch_numc_bins<int32_t>(ctx, c, crp, ccol, cval));
     CAS_TRY(scratch_free(ctx, c));
     CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[4], ctx->stream));
     CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotOvf, ctx->d_counts + kSlotOvf, sizeof(unsigned long long),
                                   cudaMemcpyDeviceToHost, ctx->stream));
+    CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotNnz, ctx->d_counts + kSlotNnz, sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
     CAS_TRY(check_status(ctx));
+    nnz = (int64_t)ctx->h_counts[kSlotNnz];
     CAS_TRY(free_owned(ctx, c.A));
     CAS_TRY(free_owned(ctx, c.B));
     return CAS_OK;
@@ -891,6 +965,17 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
         cudaEventElapsedTime(&ms, ctx->ev_numc[0][b], ctx->ev_numc[1][b]) == cudaSuccess)
       s.numc_bin_ms[b] = ms;
   }
+  s.fused_rows = c.nf;
+  s.fused_flop = c.f_flop;
+  s.fused_bytes = 0;
+  s.fused_ms = 0;
+  if (c.nf > 0) {
+    // nnz(C) of the fused rows: all entries less those of the rows with a symbolic pass
+    s.fused_bytes = (4 + vin) * ((double)c.f_nnza + (double)c.f_flop) + 12.0 * (double)(nnz - nnz_known) +
+                    16.0 * (double)c.nf;
+    float ms = 0;
+    if (ctx->profile && cudaEventElapsedTime(&ms, ctx->ev_fused[0], ctx->ev_fused[1]) == cudaSuccess) s.fused_ms = ms;
+  }
   s.esc_overflow_rows = (int64_t)(ctx->h_counts[kSlotOvf] & 0xFFFFFFFFull);
   s.esc_overflow_ms = 0;
   {
@@ -930,6 +1015,7 @@ cas_status cas_create(int device, cas_ctx** out) {
     }
     CAS_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
     for (int i = 0; i < 5; ++i) CAS_CUDA(ctx, cudaEventCreate(&ctx->ev_phase[i]));
+    for (int i = 0; i < 2; ++i) CAS_CUDA(ctx, cudaEventCreate(&ctx->ev_fused[i]));
     for (int i = 0; i < 2; ++i) {
       CAS_CUDA(ctx, cudaEventCreate(&ctx->ev_ovf[i]));
       for (int b = 0; b < cas::kSymbBins; ++b) CAS_CUDA(ctx, cudaEventCreate(&ctx->ev_symb[i][b]));
@@ -967,6 +1053,8 @@ void cas_destroy(cas_ctx* ctx) {
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   for (int i = 0; i < 5; ++i)
     if (ctx->ev_phase[i]) cudaEventDestroy(ctx->ev_phase[i]);
+  for (int i = 0; i < 2; ++i)
+    if (ctx->ev_fused[i]) cudaEventDestroy(ctx->ev_fused[i]);
   for (int i = 0; i < 2; ++i) {
     if (ctx->ev_ovf[i]) cudaEventDestroy(ctx->ev_ovf[i]);
     for (int b = 0; b < cas::kSymbBins; ++b)
@@ -1000,6 +1088,12 @@ cas_status cas_set_acc_thres(cas_ctx* ctx, double thres) {
 }
 
 const char* cas_last_error(const cas_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+cas_status cas_set_fusion(cas_ctx* ctx, int on) {
+  if (!ctx) return CAS_ERR_BAD_INPUT;
+  ctx->fuse = on != 0;
+  return CAS_OK;
+}
 
 cas_status cas_set_profiling(cas_ctx* ctx, int on) {
   if (!ctx) return CAS_ERR_BAD_INPUT;
@@ -1062,7 +1156,8 @@ cas_status cas_flp_populate(cas_ctx* ctx, const cas_csr* A, const cas_csr* B, in
   CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(cas::DevStatus), ctx->stream));
   if (c.m > 0) {
     cas::k_flp<256><<<grid_for(c.m * 32, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
-        c.A.csr, c.B.csr, c.ncol, d_row_flp, ctx->d_counts + kSlotTotals, ctx->d_counts + kSlotSymb, ctx->d_status);
+        c.A.csr, c.B.csr, c.ncol, d_row_flp, ctx->d_counts + kSlotTotals, ctx->d_counts + kSlotSymb, ctx->d_status,
+        0, ctx->d_counts + kSlotFused);
     CAS_TRY(check_launch(ctx, "k_flp"));
   }
   return check_status(ctx);

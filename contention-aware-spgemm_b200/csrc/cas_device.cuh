@@ -27,6 +27,7 @@ enum DevErr : int32_t {
   kDevCapacity = 3,      // a row reached a kernel whose shared-memory capacity it exceeds
   kDevTableFull = 4,     // hash probing did not find a free slot
   kDevBadIndex = 5,      // a column index outside [0, num_col)
+  kDevTimeout = 6,       // a bounded wait on another block gave up
 };
 
 struct DevStatus {

@@ -12,10 +12,12 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_flp(Csr A, Csr B, int64_t c_ncol, int64_t* __restrict__ row_flp,
       unsigned long long* __restrict__ totals, unsigned long long* __restrict__ bin_count,
-      DevStatus* st) {
+      DevStatus* st, int fuse, unsigned long long* __restrict__ fused_sums) {
   __shared__ unsigned long long s_cnt[kSymbBins];
-  __shared__ unsigned long long s_tot, s_max;
+  __shared__ unsigned long long s_tot, s_max, s_f[4];
+  unsigned long long my_f[4] = {0, 0, 0, 0};
   if (threadIdx.x < kSymbBins) s_cnt[threadIdx.x] = 0;
+  if (threadIdx.x < 4) s_f[threadIdx.x] = 0;
   if (threadIdx.x == 0) { s_tot = 0; s_max = 0; }
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -37,15 +39,24 @@ k_flp(Csr A, Csr B, int64_t c_ncol, int64_t* __restrict__ row_flp,
       row_flp[r] = sum;
       my_tot += (unsigned long long)sum;
       my_max = max(my_max, (unsigned long long)sum);
-      atomicAdd(&s_cnt[symb_bin_of(sum, c_ncol)], 1ull);
+      atomicAdd(&s_cnt[symb_bin_of(sum, c_ncol, fuse)], 1ull);
+      if (fused_row(sum, fuse)) {  // fused rows: count, products, output bound, nnz(A)
+        my_f[0] += 1;
+        my_f[1] += (unsigned long long)sum;
+        my_f[2] += (unsigned long long)(sum < c_ncol ? sum : c_ncol);
+        my_f[3] += (unsigned long long)(e - s);
+      }
     }
   }
+  if (lane == 0 && my_f[0])
+    for (int i = 0; i < 4; ++i) atomicAdd(&s_f[i], my_f[i]);
   if (lane == 0) {
     atomicAdd(&s_tot, my_tot);
     atomicMax(&s_max, my_max);
   }
   __syncthreads();
   if (threadIdx.x < kSymbBins && s_cnt[threadIdx.x]) atomicAdd(&bin_count[threadIdx.x], s_cnt[threadIdx.x]);
+  if (threadIdx.x < 4 && s_f[threadIdx.x]) atomicAdd(&fused_sums[threadIdx.x], s_f[threadIdx.x]);
   if (threadIdx.x == 0) {
     atomicAdd(&totals[0], s_tot);
     atomicMax(&totals[1], s_max);
@@ -55,12 +66,23 @@ k_flp(Csr A, Csr B, int64_t c_ncol, int64_t* __restrict__ row_flp,
 // Rows into per-bin lists.  cursor[b] starts at the bin's offset; lanes that
 // hit the same bin share one atomic (warp-aggregated).
 __global__ void k_bin_scatter_symb(int64_t m, const int64_t* __restrict__ row_flp, int64_t c_ncol,
-                                   unsigned long long* __restrict__ cursor, int32_t* __restrict__ rows) {
+                                   unsigned long long* __restrict__ cursor, int32_t* __restrict__ rows, int fuse) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
-    const int b = symb_bin_of(row_flp[r], c_ncol);
+    const int b = symb_bin_of(row_flp[r], c_ncol, fuse);
     const unsigned long long pos = warp_aggregated_add(cursor, b);
     rows[pos] = (int32_t)r;
   }
+}
+
+// Fused rows in ascending order: a 0/1 mark per row, scanned, then scattered.
+__global__ void k_fused_mark(int64_t m, const int64_t* __restrict__ row_flp, int fuse, int64_t* __restrict__ mark) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x)
+    mark[r] = fused_row(row_flp[r], fuse) ? 1 : 0;
+}
+__global__ void k_fused_scatter(int64_t m, const int64_t* __restrict__ row_flp, int fuse,
+                                const int64_t* __restrict__ pos, int32_t* __restrict__ frows) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x)
+    if (fused_row(row_flp[r], fuse)) frows[pos[r]] = (int32_t)r;
 }
 
 // Numeric bin histogram plus, per bin, the sums of products, nnz(C) and
@@ -902,11 +924,77 @@ __device__ __forceinline__ int warp_sort_compact(uint32_t* __restrict__ skey, AT
 constexpr int kBucketLimit = 128;
 constexpr int kBigBuckets = 64;  // buckets of more than 8 pairs one row may have
 
-template <int BLOCK, int CAP, int NBB, typename VIn>
+// ---- fused rows: count and place in one pass -------------------------------
+// The fused form of the kernel runs the rows of one product-count range
+// without a symbolic pass.  Each block takes the next row in row order from
+// a ticket counter, counts the row's distinct columns, and finds where the
+// row goes in C from the counts of the earlier fused rows by a decoupled
+// look-back (Merrill & Garland, "Single-pass Parallel Prefix Scan with
+// Decoupled Look-back", 2016) over one status word per fused row, plus the
+// known counts of all other rows before it.  A block waits only for rows
+// with an earlier ticket, whose blocks are already running, so the chain
+// always advances; every wait is bounded all the same and gives up with an
+// error status instead of hanging.
+struct Fused {
+  const int32_t* rows;              // fused rows, ascending
+  unsigned long long* ticket;       // next ticket
+  unsigned long long* status;       // one look-back word per fused row, zeroed
+  const int64_t* known;             // exclusive prefix of the counts of the other rows
+  int64_t* row_nz;                  // out: each fused row's count
+  int64_t cap;                      // entries C has room for
+};
+constexpr unsigned long long kLbAgg = 1ull << 62;   // the word holds the row's own count
+constexpr unsigned long long kLbInc = 2ull << 62;   // the word holds the inclusive prefix
+constexpr unsigned long long kLbVal = (1ull << 62) - 1;
+constexpr int kLbSpins = 1 << 22;                   // polls (about 64 ns apart) before giving up
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Warp 0 of the block holding ticket t: publishes `count`, returns the sum of
+// the counts of all earlier tickets, or -1 when a wait gave up.
+__device__ long long lookback_prefix(unsigned long long* status, int64_t t, long long count) {
+  const int lane = threadIdx.x & 31;
+  if (t == 0) {
+    if (lane == 0) st_release_u64(&status[0], kLbInc | (unsigned long long)count);
+    return 0;
+  }
+  if (lane == 0) st_release_u64(&status[t], kLbAgg | (unsigned long long)count);
+  long long excl = 0;
+  int64_t j = t - 1;
+  int spins = 0;
+  for (;;) {
+    const int64_t idx = j - lane;
+    const unsigned long long v = idx >= 0 ? ld_acquire_u64(&status[idx]) : kLbInc;
+    if (__any_sync(kFull, (v >> 62) == 0)) {
+      if (++spins > kLbSpins) return -1;
+      __nanosleep(64);
+      continue;
+    }
+    const unsigned inc = __ballot_sync(kFull, (v >> 62) == 2);
+    const int stop = inc ? __ffs(inc) - 1 : 31;
+    long long part = lane <= stop ? (long long)(v & kLbVal) : 0;
+    excl += warp_sum(part);
+    if (inc) break;
+    j -= 32;
+  }
+  if (lane == 0) st_release_u64(&status[t], kLbInc | (unsigned long long)(excl + count));
+  return excl;
+}
+
+__host__ __device__ constexpr int floor_pow2(int x) { return x < 2 ? 1 : 2 * floor_pow2(x / 2); }
+
+template <int BLOCK, int CAP, int NBB, typename VIn, bool FUSED = false>
 __global__ void __launch_bounds__(BLOCK)
 k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted, const int64_t* __restrict__ crp,
                int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval,
-               int32_t* __restrict__ ovf, unsigned int* __restrict__ ovf_count, DevStatus* st) {
+               int32_t* __restrict__ ovf, unsigned int* __restrict__ ovf_count, DevStatus* st, Fused fu) {
   using AT = typename Acc<VIn>::T;
   constexpr int NB = 1 << NBB;
   constexpr int NW = BLOCK / 32;
@@ -923,9 +1011,61 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   uint32_t* ccnt = bcnt + NB / 2;     // NCH chunk counts / offsets
   uint8_t* segof = reinterpret_cast<uint8_t*>(ccnt + NCH);
   StageB<VIn>& sg = *reinterpret_cast<StageB<VIn>*>(segof + ((CAP + 15) & ~15));
-  const int64_t r = rows[blockIdx.x];
+  __shared__ long long s_tick, s_off;
+  int64_t r, tick = 0;
+  if (FUSED) {
+    if (threadIdx.x == 0) s_tick = (long long)atomicAdd(fu.ticket, 1ull);
+    __syncthreads();
+    tick = s_tick;
+    r = fu.rows[tick];
+  } else {
+    r = rows[blockIdx.x];
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t as = A.rp[r], ae = A.rp[r + 1];
+  // fused rows: publish `cnt` and return the row's first position in C (-1
+  // when the look-back gave up)
+  auto place = [&](long long cnt) -> long long {
+    if (warp == 0) {
+      const long long ex = lookback_prefix(fu.status, tick, cnt);
+      if (lane == 0) {
+        s_off = ex < 0 ? -1 : (long long)fu.known[r] + ex;
+        fu.row_nz[r] = ex < 0 ? 0 : cnt;
+        if (ex < 0) dev_report(st, kDevTimeout, 15, r);
+      }
+    }
+    __syncthreads();
+    return s_off;
+  };
+  // fused rows whose buckets overflow: the distinct count from a hash over the
+  // whole shared arena, published so that later rows can go on; the row itself
+  // is left to the radix-sort ESC kernel, which writes it at its place
+  auto count_and_defer = [&]() {
+    constexpr int TS = floor_pow2(CAP * (int)(sizeof(AT) + 4) / 4);
+    constexpr int TB = __builtin_ctz(TS);
+    uint32_t* tab = reinterpret_cast<uint32_t*>(smem);
+    __syncthreads();
+    for (int i = threadIdx.x; i < TS; i += BLOCK) tab[i] = kEmptyKey;
+    __syncthreads();
+    int cnt = 0;
+    for (int64_t a0 = as; a0 < ae; a0 += ACH) {
+      const int na = (int)((ae - a0) < (int64_t)ACH ? (ae - a0) : (int64_t)ACH);
+      const int t = stage_chunk<BLOCK, false, VIn>(A, B, a0, na, sg, segof, CAP, false);
+      expand_chunk<BLOCK, false, VIn>(B, t, sg, segof, [&](int32_t key, VIn, VIn, int) {
+        uint32_t h = hash_slot((uint32_t)key, TB);
+        for (int probe = 0; probe < TS; ++probe) {
+          const uint32_t old = atomicCAS(&tab[h], kEmptyKey, (uint32_t)key);
+          if (old == kEmptyKey) { ++cnt; return; }
+          if (old == (uint32_t)key) return;
+          h = (h + 1) & (TS - 1);
+        }
+      });
+      __syncthreads();
+    }
+    const int distinct = block_sum<BLOCK, int>(cnt, sg.tmp);
+    place(distinct);
+    if (threadIdx.x == 0) ovf[atomicAdd(ovf_count, 1u)] = (int32_t)r;
+  };
   if (threadIdx.x == 0) { sg.kmin = 0xFFFFFFFFu; sg.kmax = 0u; sg.over = 0; }
   for (int i = threadIdx.x; i < NB / 2; i += BLOCK) bcnt[i] = 0u;
   // the column range: from the staged chunk when the row has one chunk,
@@ -967,6 +1107,7 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
     total = stage_chunk<BLOCK, true, VIn>(A, B, a0, na, sg, segof, CAP - n, one_chunk && b_sorted);
     if (n + total > CAP) {  // uniform: the bin bound was violated
       if (threadIdx.x == 0) dev_report(st, kDevCapacity, 14, r);
+      if (FUSED) place(0);
       return;
     }
     lo = sg.kmin;
@@ -992,7 +1133,8 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
       big = max(big, max(c0, c1));
     }
     if (__syncthreads_or(big > (uint32_t)kBucketLimit)) {
-      if (threadIdx.x == 0) ovf[atomicAdd(ovf_count, 1u)] = (int32_t)r;
+      if (FUSED) count_and_defer();
+      else if (threadIdx.x == 0) ovf[atomicAdd(ovf_count, 1u)] = (int32_t)r;
       return;
     }
     int tot_all;
@@ -1046,7 +1188,8 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   }
   __syncthreads();
   if (s_nbig > kBigBuckets) {  // uniform: too many large buckets for this form
-    if (threadIdx.x == 0) ovf[atomicAdd(ovf_count, 1u)] = (int32_t)r;
+    if (FUSED) count_and_defer();
+    else if (threadIdx.x == 0) ovf[atomicAdd(ovf_count, 1u)] = (int32_t)r;
     return;
   }
   for (int i = warp; i < s_nbig; i += NW) {
@@ -1071,7 +1214,19 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
     if (threadIdx.x < nch) ccnt[threadIdx.x] = (uint32_t)ex;
   }
   __syncthreads();
-  const int64_t c0 = crp[r], nz = crp[r + 1] - c0;
+  int64_t c0, nz;
+  if (FUSED) {
+    c0 = place(distinct);
+    if (c0 < 0) return;
+    nz = distinct;
+    if (c0 + nz > fu.cap) {
+      if (threadIdx.x == 0) dev_report(st, kDevRowOverflow, 15, r);
+      return;
+    }
+  } else {
+    c0 = crp[r];
+    nz = crp[r + 1] - c0;
+  }
   for (int c = warp; c < nch; c += NW) {
     const int t = c * 32 + lane;
     uint32_t key = kEmptyKey;
@@ -1086,7 +1241,8 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
       }
     }
   }
-  if (threadIdx.x == 0 && distinct != nz) dev_report(st, distinct > nz ? kDevRowOverflow : kDevRowUnderflow, 14, r);
+  if (!FUSED && threadIdx.x == 0 && distinct != nz)
+    dev_report(st, distinct > nz ? kDevRowOverflow : kDevRowUnderflow, 14, r);
 }
 
 // Hash accumulator for rows with at most 2^TBITS / 2 distinct columns: linear

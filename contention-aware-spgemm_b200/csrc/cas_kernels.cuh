@@ -70,8 +70,15 @@ struct Csr {
   const void* __restrict__ val;
 };
 
-__host__ __device__ __forceinline__ int symb_bin_of(int64_t flp, int64_t ncol) {
-  if (flp <= 0) return kSB_Zero;
+// Rows with kFusedLo < products <= kFusedHi run through the fused ESC kernel
+// when fusion is on: no symbolic pass, so they sit in the symbolic zero bin.
+constexpr int64_t kFusedLo = 2048;
+constexpr int64_t kFusedHi = 4800;
+__host__ __device__ __forceinline__ bool fused_row(int64_t flp, int fuse) {
+  return fuse && flp > kFusedLo && flp <= kFusedHi;
+}
+__host__ __device__ __forceinline__ int symb_bin_of(int64_t flp, int64_t ncol, int fuse = 0) {
+  if (flp <= 0 || fused_row(flp, fuse)) return kSB_Zero;
   if (flp <= 32) return kSB_Tiny;
   const int64_t t = flp < ncol ? flp : ncol;
   if (t <= 512) return kSB_H1K;

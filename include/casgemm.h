@@ -99,6 +99,12 @@ typedef struct {
 	 * columns crowd into a narrow range), and that kernel's time (profiling) */
 	int64_t esc_overflow_rows;
 	double esc_overflow_ms;
+	/* rows of the fused ESC kernel (no symbolic pass; see cas_set_fusion),
+	 * their products and algorithmic bytes (as above), its time (profiling) */
+	int64_t fused_rows;
+	int64_t fused_flop;
+	double fused_bytes;
+	double fused_ms;
 } cas_stats;
 
 typedef struct cas_ctx cas_ctx;
@@ -113,6 +119,13 @@ cas_status cas_set_stream(cas_ctx *ctx, void *stream);
  * script's value for ams_hybaccspgemm (scripts/ams_rmat_run.sh:33). */
 cas_status cas_set_acc_thres(cas_ctx *ctx, double thres);
 const char *cas_last_error(const cas_ctx *ctx);
+/* 1 (default): in cas_spgemm with the ESC or hybrid accumulator, rows of
+ * 2049..4800 products skip the symbolic pass: one kernel counts, sorts and
+ * places each of them, finding its offset in C from the rows before it, and
+ * C is allocated by the bound min(products, columns) for those rows
+ * (C->num_nnz is exact; the arrays may be longer).  0: every row has a
+ * symbolic pass, as in the reference's drivers.  The output is the same. */
+cas_status cas_set_fusion(cas_ctx *ctx, int on);
 /* 1: run the bins one after another on the context's stream and time every
  * bin kernel with CUDA events (cas_stats.*_bin_ms); 0 (default): bins run
  * concurrently on auxiliary streams. */

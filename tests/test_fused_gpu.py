@@ -1,0 +1,115 @@
+"""GPU: the fused ESC rows (no symbolic pass, offsets by look-back).
+
+Rows of 2049..4800 products are counted, sorted and placed by one kernel in
+row order.  Checked bit for bit against the oracle and against the same
+product with fusion off: uniform rows (nearly all fused), rows whose
+buckets overflow (deferred to the radix-sort kernel after an in-kernel
+count), int32 values, rows split over several A chunks, device output.
+"""
+import numpy as np
+import pytest
+
+import casgemm
+import oracle
+from matrices import from_coo, with_int_values
+
+pytestmark = pytest.mark.gpu
+
+
+def same(out, ref):
+    np.testing.assert_array_equal(out.csr.row_ptrs, ref[0])
+    np.testing.assert_array_equal(out.csr.cols.astype(np.int64), ref[1])
+    np.testing.assert_array_equal(out.csr.vals.astype(np.float64), ref[2])
+
+
+def hot_column_matrix(seed=3):
+    """Rows whose products crowd one bucket: 160 A entries whose B rows all
+    hold column 0 (so 160 equal keys), plus a narrow band of distinct columns."""
+    rng = np.random.default_rng(seed)
+    n_rows, n_mid = 40, 400
+    r, c = [], []
+    for i in range(n_rows):
+        ks = rng.choice(n_mid, 160, replace=False)
+        r += [i] * 160
+        c += list(ks)
+    A = from_coo(n_rows, n_mid, np.array(r), np.array(c))
+    br, bc = [], []
+    for k in range(n_mid):
+        cols = np.concatenate([[0], rng.choice(np.arange(1, 3000), 19, replace=False)])
+        br += [k] * 20
+        bc += list(cols)
+    B = from_coo(n_mid, 3000, np.array(br), np.array(bc))
+    return A, B
+
+
+@pytest.mark.parametrize("algo", ["hybacc", "hsersc"])
+def test_er_rows_fused(ctx, algo):
+    A = casgemm.gen_er(13, 32, 7)
+    B = A.transpose()
+    ref = oracle.oracle_spgemm(A, B, algo)
+    out = ctx.spgemm(A, B, algo)
+    assert out.stats["fused_rows"] > A.num_row // 2
+    same(out, ref)
+    ctx.set_fusion(False)
+    try:
+        off = ctx.spgemm(A, B, algo)
+    finally:
+        ctx.set_fusion(True)
+    assert off.stats["fused_rows"] == 0
+    same(off, ref)
+
+
+def test_overflowing_fused_rows_are_deferred(ctx):
+    A, B = hot_column_matrix()
+    ref = oracle.oracle_spgemm(A, B, "hybacc")
+    out = ctx.spgemm(A, B, "hybacc")
+    assert out.stats["fused_rows"] == A.num_row
+    assert out.stats["esc_overflow_rows"] == A.num_row
+    same(out, ref)
+
+
+def test_fused_int_values(ctx):
+    A = with_int_values(casgemm.gen_g500(12, 16, 5), 9)
+    B = A.transpose()
+    ref = oracle.oracle_spgemm(A, B, "hybacc")
+    out = ctx.spgemm(A, B, "hybacc")
+    assert out.stats["fused_rows"] > 0
+    assert out.csr.vals.dtype == np.int64
+    same(out, ref)
+
+
+def test_fused_rows_over_several_a_chunks(ctx):
+    """A rows of 200 entries (the kernel stages 128 at a time), 15 per B row."""
+    rng = np.random.default_rng(8)
+    r = np.repeat(np.arange(30), 200)
+    c = np.concatenate([rng.choice(1000, 200, replace=False) for _ in range(30)])
+    A = from_coo(30, 1000, r, c, rng.integers(1, 5, len(r)).astype(np.float64))
+    br = np.repeat(np.arange(1000), 15)
+    bc = np.concatenate([rng.choice(5000, 15, replace=False) for _ in range(1000)])
+    B = from_coo(1000, 5000, br, bc, rng.integers(1, 5, len(br)).astype(np.float64))
+    ref = oracle.oracle_spgemm(A, B, "hybacc")
+    out = ctx.spgemm(A, B, "hybacc")
+    assert out.stats["fused_rows"] == 30
+    same(out, ref)
+
+
+def test_fused_device_output_digest(ctx):
+    import torch
+    dev = torch.device("cuda", 0)
+    A = casgemm.gen_er(12, 32, 11)
+    B = A.transpose()
+
+    def to_dev(M):
+        t = [torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in (M.row_ptrs, M.cols, M.vals)]
+        return casgemm.DeviceCsr(M.num_row, M.num_col, M.nnz, t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(),
+                                 M.val_type, keep=t)
+
+    cc, _ = ctx.spgemm_device(to_dev(A), to_dev(B), "hybacc")
+    try:
+        d = ctx.digest(cc)
+        nnz = cc.num_nnz
+    finally:
+        ctx.free(cc)
+    rp, cols, vals, _ = oracle.oracle_spgemm(A, B, "hybacc")
+    assert nnz == len(cols)
+    assert d == oracle.csr_digest(rp, cols, vals)[0]
