@@ -509,7 +509,7 @@ def main():
     dom_bytes = bin_bytes[dom]
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9 if dom_ms > 0 else 0.0
     kernel_name = {"tiny": "k_numc_tiny<256>", "hash256": "k_numc_hash<256,9>", "hash1k": "k_numc_hash<256,11>",
-                   "hash4k": "k_numc_hash<512,13>", "dense": "k_numc_dense<1024>"}.get(dom)
+                   "hash4k": "k_numc_hash<512,13>", "dense": "k_numc_dense<512>"}.get(dom)
     if dom == "fused":
         kernel_name = "k_numc_esc_msd<256,4800,11,fused>"
     if kernel_name is None and dom.startswith("esc"):

@@ -164,8 +164,7 @@ constexpr size_t smem_numc_hash() {
 }
 template <int BLOCK, typename VIn>
 constexpr size_t smem_numc_dense() {
-  return size_t(cas::kDenseChunkCols) * sizeof(typename cas::Acc<VIn>::T) + size_t(cas::kDenseChunkCols / 32) * 4 +
-         sizeof(cas::Stage<VIn>);
+  return size_t(cas::kRankCols / 32) * 8 + sizeof(cas::Stage<VIn>);
 }
 
 template <int CAP, int NBB, typename VIn>
@@ -209,7 +208,7 @@ cas_status setup_numc_kernels(cas_ctx* ctx) {
   CAS_TRY(allow_smem(ctx, k_numc_hash<256, 9, VIn>, smem_numc_hash<256, 9, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_hash<256, 11, VIn>, smem_numc_hash<256, 11, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_hash<512, 13, VIn>, smem_numc_hash<512, 13, VIn>()));
-  CAS_TRY(allow_smem(ctx, k_numc_dense<1024, VIn>, smem_numc_dense<1024, VIn>()));
+  CAS_TRY(allow_smem(ctx, k_numc_dense<512, VIn>, smem_numc_dense<512, VIn>()));
   return CAS_OK;
 }
 
@@ -776,9 +775,9 @@ cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* 
         k_numc_hash<512, 13, VIn><<<(unsigned)n, 512, smem_numc_hash<512, 13, VIn>(), s>>>(rows, A, B, crp, ccol, cval, ctx->d_status);
         break;
       case kNB_Dense:
-        if (!c.b_sorted && c.ncol > kDenseChunkCols)
-          return set_err(ctx, CAS_ERR_BAD_INPUT, "heavy rows over more than %d columns need B rows sorted by column", kDenseChunkCols);
-        k_numc_dense<1024, VIn><<<(unsigned)n, 1024, smem_numc_dense<1024, VIn>(), s>>>(
+        if (!c.b_sorted && c.ncol > kRankCols)
+          return set_err(ctx, CAS_ERR_BAD_INPUT, "heavy rows over more than %d columns need B rows sorted by column", kRankCols);
+        k_numc_dense<512, VIn><<<(unsigned)n, 512, smem_numc_dense<512, VIn>(), s>>>(
             rows, A, B, c.ncol, c.b_sorted ? 1 : 0, crp, ccol, cval, ctx->d_status);
         break;
     }
@@ -961,7 +960,7 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
     s.numc_bin_bytes[b] = (4 + vin) * (nza + flp) + 12.0 * nzc + 16.0 * (double)c.numc_count[b];
     s.numc_bin_ms[b] = 0;
     float ms = 0;
-    if (ctx->profile && c.numc_count[b] > 0 &&
+    if (ctx->profile && b != kNB_Zero && c.numc_count[b] > 0 &&
         cudaEventElapsedTime(&ms, ctx->ev_numc[0][b], ctx->ev_numc[1][b]) == cudaSuccess)
       s.numc_bin_ms[b] = ms;
   }
@@ -986,10 +985,11 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
   for (int b = 0; b < kSymbBins; ++b) {
     s.symb_bin_ms[b] = 0;
     float ms = 0;
-    if (ctx->profile && c.symb_count[b] > 0 &&
+    if (ctx->profile && b != kSB_Zero && c.symb_count[b] > 0 &&
         cudaEventElapsedTime(&ms, ctx->ev_symb[0][b], ctx->ev_symb[1][b]) == cudaSuccess)
       s.symb_bin_ms[b] = ms;
   }
+  cudaGetLastError();  // leave no error pending from the timing queries
   return CAS_OK;
 }
 

@@ -1329,56 +1329,78 @@ k_numc_hash(const int32_t* __restrict__ rows, Csr A, Csr B, const int64_t* __res
   if (threadIdx.x == 0 && n != nz) dev_report(st, n > nz ? kDevRowOverflow : kDevRowUnderflow, 12, r);
 }
 
-// Heavy rows: dense accumulation over kDenseChunkCols columns at a time
-// (values plus a presence bitmap in shared memory), written in column order
-// straight from the chunk, so no sort is needed.  B rows are cut to each
-// chunk by binary search (B rows sorted by column).
+// Heavy rows in one pass per slice of kRankCols columns of the row's column
+// range: a keys-only expansion marks the row's columns in a shared-memory
+// bitmap, an exclusive scan of the words' population counts ranks every
+// column, the column indices are written to C from the bitmap and the values
+// zeroed, and a second expansion adds every product straight into its place
+// in C with a global atomic add (resolved in L2: a row's values are at most
+// 8 bytes x nnz(row) there).  Shared memory holds 2 bits per column, so four
+// 512-thread blocks fit an SM; a range wider than one slice is cut into
+// slices, B rows cut to each by binary search (B rows sorted).
+constexpr int kRankCols = 1 << 17;  // columns per slice: 16 KiB bitmap + 16 KiB word ranks
+
 template <int BLOCK, typename VIn>
 __global__ void __launch_bounds__(BLOCK)
 k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int32_t b_sorted,
              const int64_t* __restrict__ crp, int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval,
              DevStatus* st) {
   using AT = typename Acc<VIn>::T;
-  constexpr int CW = kDenseChunkCols;
-  constexpr int NWORD = CW / 32;
-  static_assert(NWORD <= BLOCK, "one bitmap word per thread");
+  constexpr int NWORD = kRankCols / 32;
   extern __shared__ __align__(16) uint8_t smem[];
-  AT* dv = reinterpret_cast<AT*>(smem);
-  uint32_t* bm = reinterpret_cast<uint32_t*>(dv + CW);
-  Stage<VIn>& sg = *reinterpret_cast<Stage<VIn>*>(reinterpret_cast<uint8_t*>(bm + NWORD));
+  uint32_t* bm = reinterpret_cast<uint32_t*>(smem);
+  uint32_t* rank = bm + NWORD;
+  Stage<VIn>& sg = *reinterpret_cast<Stage<VIn>*>(reinterpret_cast<uint8_t*>(rank + NWORD));
   const int64_t r = rows[blockIdx.x];
   const int64_t c0r = crp[r], nz = crp[r + 1] - c0r;
   int64_t lo, hi;
   row_col_range<BLOCK>(A, B, r, b_sorted != 0, c_ncol, lo, hi);
-  const bool multi = hi - lo > CW;
+  const bool multi = hi - lo > kRankCols;
   int64_t written = 0;
-  for (int64_t c0 = lo; c0 < hi; c0 += CW) {
-    const int64_t c1 = (hi < c0 + CW ? hi : c0 + CW);
-    for (int i = threadIdx.x; i < CW; i += BLOCK) dv[i] = AT(0);
-    for (int i = threadIdx.x; i < NWORD; i += BLOCK) bm[i] = 0u;
+  for (int64_t s0 = lo; s0 < hi; s0 += kRankCols) {
+    const int64_t s1 = hi < s0 + kRankCols ? hi : s0 + kRankCols;
+    const int nw = (int)((s1 - s0 + 31) >> 5);
+    for (int i = threadIdx.x; i < nw; i += BLOCK) bm[i] = 0u;
     __syncthreads();
-    expand_row<BLOCK, true, VIn>(A, B, r, sg, multi, (int32_t)c0, (int32_t)c1,
-                                 [&](int32_t key, VIn av, VIn bv, int64_t) {
-      const int64_t idx = (int64_t)key - c0;
-      if (idx < 0 || idx >= CW) return;
-      atomicOr(&bm[idx >> 5], 1u << (idx & 31));
-      Acc<VIn>::atomic_add(&dv[idx], Acc<VIn>::mul(av, bv));
+    expand_row<BLOCK, false, VIn>(A, B, r, sg, multi, (int32_t)s0, (int32_t)s1, [&](int32_t key, VIn, VIn, int64_t) {
+      const int64_t idx = (int64_t)key - s0;
+      if (idx >= 0 && idx < kRankCols) atomicOr(&bm[idx >> 5], 1u << (idx & 31));
     });
     __syncthreads();
-    uint32_t word = threadIdx.x < NWORD ? bm[threadIdx.x] : 0u;
-    long long tot;
-    const long long ex = block_exclusive_sum<BLOCK, long long>((long long)__popc(word), sg.tmp, tot);
-    int64_t pos = written + ex;
-    while (word) {
-      const int b = __ffs(word) - 1;
-      word &= word - 1;
-      if (pos < nz) {
-        ccol[c0r + pos] = (int32_t)(c0 + threadIdx.x * 32 + b);
-        cval[c0r + pos] = dv[threadIdx.x * 32 + b];
-      }
-      ++pos;
+    long long run = 0;
+    for (int w0 = 0; w0 < nw; w0 += BLOCK) {
+      const int w = w0 + threadIdx.x;
+      long long tot;
+      const long long ex = block_exclusive_sum<BLOCK, long long>(w < nw ? (long long)__popc(bm[w]) : 0ll, sg.tmp, tot);
+      if (w < nw) rank[w] = (uint32_t)(run + ex);
+      run += tot;
     }
-    written += tot;
+    __syncthreads();
+    const int64_t base = c0r + written;
+    const int64_t room = nz - written;  // guards the writes if the counts disagree
+    for (int w = threadIdx.x; w < nw; w += BLOCK) {
+      uint32_t word = bm[w];
+      int64_t pos = rank[w];
+      while (word) {
+        const int b = __ffs(word) - 1;
+        word &= word - 1;
+        if (pos < room) {
+          ccol[base + pos] = (int32_t)(s0 + w * 32 + b);
+          cval[base + pos] = AT(0);
+        }
+        ++pos;
+      }
+    }
+    __syncthreads();  // the zeroed values are visible to the block's atomic adds
+    expand_row<BLOCK, true, VIn>(A, B, r, sg, multi, (int32_t)s0, (int32_t)s1,
+                                 [&](int32_t key, VIn av, VIn bv, int64_t) {
+      const int64_t idx = (int64_t)key - s0;
+      if (idx < 0 || idx >= kRankCols) return;
+      const int w = (int)(idx >> 5);
+      const int64_t pos = rank[w] + __popc(bm[w] & ((1u << (idx & 31)) - 1u));
+      if (pos < room) Acc<VIn>::atomic_add(&cval[base + pos], Acc<VIn>::mul(av, bv));
+    });
+    written += run;
     __syncthreads();
   }
   if (threadIdx.x == 0 && written != nz) dev_report(st, written > nz ? kDevRowOverflow : kDevRowUnderflow, 13, r);

@@ -61,7 +61,6 @@ enum NumcBin : int {
 enum AccumMode : int { kAccHash = 0, kAccEsc = 1, kAccHybrid = 2 };
 
 constexpr int kDenseChunkBits = 1 << 20;   // symbolic bitmap chunk: 1 Mi columns (128 KiB)
-constexpr int kDenseChunkCols = 16384;     // numeric dense chunk: 16 Ki columns (128 KiB of values)
 
 struct Csr {
   int64_t nrow, ncol;

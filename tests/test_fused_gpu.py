@@ -113,3 +113,17 @@ def test_fused_device_output_digest(ctx):
     rp, cols, vals, _ = oracle.oracle_spgemm(A, B, "hybacc")
     assert nnz == len(cols)
     assert d == oracle.csr_digest(rp, cols, vals)[0]
+
+
+def test_profiling_leaves_no_cuda_error(ctx):
+    """Timing queries for bins that never ran must not leave an error behind
+    (the next CUDA call of another library would report it)."""
+    import torch
+    A = casgemm.gen_er(12, 32, 3)
+    ctx.set_profiling(True)
+    try:
+        out = ctx.spgemm(A, A.transpose(), "hybacc")
+    finally:
+        ctx.set_profiling(False)
+    assert out.stats["fused_rows"] > 0 and out.stats["fused_ms"] > 0
+    torch.zeros(4, device="cuda").sum().item()  # raises if an error is pending
