@@ -217,7 +217,7 @@ cas_status setup_kernels(cas_ctx* ctx) {
 #define CAS_SETUP_SYMB(bin, BLK, TB, SEG) CAS_TRY(allow_smem(ctx, k_symb_hash<BLK, TB, SEG>, smem_symb_hash<BLK, TB, SEG>()));
   CAS_SYMB_SHAPES(CAS_SETUP_SYMB)
 #undef CAS_SETUP_SYMB
-  CAS_TRY(allow_smem(ctx, k_symb_dense<1024>, smem_symb_dense<1024>()));
+  CAS_TRY(allow_smem(ctx, k_symb_dense<512>, smem_symb_dense<512>()));
   CAS_TRY(setup_numc_kernels<double>(ctx));
   CAS_TRY(setup_numc_kernels<int32_t>(ctx));
   return CAS_OK;
@@ -685,7 +685,7 @@ cas_status launch_symb_bins(cas_ctx* ctx, Call& c, int64_t* row_nz) {
       case kSB_Dense:
         if (!c.b_sorted && c.ncol > kDenseChunkBits)
           return set_err(ctx, CAS_ERR_BAD_INPUT, "heavy rows over more than %d columns need B rows sorted by column", kDenseChunkBits);
-        k_symb_dense<1024><<<(unsigned)n, 1024, smem_symb_dense<1024>(), s>>>(rows, c.A.csr, c.B.csr, c.ncol,
+        k_symb_dense<512><<<(unsigned)n, 512, smem_symb_dense<512>(), s>>>(rows, c.A.csr, c.B.csr, c.ncol,
                                                                             c.b_sorted ? 1 : 0, row_nz, ctx->d_status);
         break;
     }

@@ -395,7 +395,8 @@ k_symb_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int
   long long cnt = 0;
   for (int64_t c0 = lo; c0 < hi; c0 += kDenseChunkBits) {
     const int64_t c1 = (hi < c0 + kDenseChunkBits ? hi : c0 + kDenseChunkBits);
-    for (int i = threadIdx.x; i < W; i += BLOCK) bm[i] = 0u;
+    const int nw = (int)((c1 - c0 + 31) >> 5);  // words the slice uses
+    for (int i = threadIdx.x; i < nw; i += BLOCK) bm[i] = 0u;
     __syncthreads();
     bool bad = false;
     expand_row<BLOCK, false, double>(A, B, r, sg, multi, (int32_t)c0, (int32_t)c1,
@@ -406,7 +407,7 @@ k_symb_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int
     });
     if (bad && !multi) dev_report(st, kDevBadIndex, 3, r);
     __syncthreads();
-    for (int i = threadIdx.x; i < W; i += BLOCK) cnt += __popc(bm[i]);
+    for (int i = threadIdx.x; i < nw; i += BLOCK) cnt += __popc(bm[i]);
     __syncthreads();
   }
   cnt = block_sum<BLOCK, long long>(cnt, sg.tmp);

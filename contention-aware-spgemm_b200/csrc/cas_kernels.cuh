@@ -60,7 +60,7 @@ enum NumcBin : int {
 
 enum AccumMode : int { kAccHash = 0, kAccEsc = 1, kAccHybrid = 2 };
 
-constexpr int kDenseChunkBits = 1 << 20;   // symbolic bitmap chunk: 1 Mi columns (128 KiB)
+constexpr int kDenseChunkBits = 1 << 18;   // symbolic bitmap slice: 256 Ki columns (32 KiB)
 
 struct Csr {
   int64_t nrow, ncol;
