@@ -46,6 +46,7 @@ constexpr int kSlotBinSums = 64; // [64, 103) per numeric bin: products, nnz(C),
 constexpr int kSlotOvf = 110;    // [110]   rows handed to the radix-sort ESC kernel
 constexpr int kSlotFused = 112;  // [112, 116) fused rows: count, products, output bound, nnz(A); [116] ticket
 constexpr size_t kStageBytes = size_t(64) << 20;  // pinned staging chunk for host copies
+constexpr double kSavedBitmapBytes = 8.0 * (1ull << 30);  // heavy-row bitmaps kept between the phases
 
 }  // namespace
 
@@ -509,6 +510,9 @@ struct Call {
   int64_t* fpos = nullptr;
   unsigned long long* fstatus = nullptr;
   bool ovf_preset = false;
+  // bitmaps of heavy rows kept by the symbolic kernel for the numeric one
+  uint32_t* dbits = nullptr;
+  int32_t* dslot = nullptr;
 };
 
 cas_status fork(cas_ctx* ctx) {
@@ -535,7 +539,7 @@ cas_status scratch_alloc(cas_ctx* ctx, Call& c) {
 }
 
 cas_status scratch_free(cas_ctx* ctx, Call& c) {
-  void* ps[] = {c.row_flp, c.row_nz, c.rows, c.ovf, c.partial, c.frows, c.fpos, c.fstatus};
+  void* ps[] = {c.row_flp, c.row_nz, c.rows, c.ovf, c.partial, c.frows, c.fpos, c.fstatus, c.dbits, c.dslot};
   for (void* p : ps)
     if (p) CAS_CUDA(ctx, cudaFreeAsync(p, ctx->stream));
   c.row_flp = c.row_nz = nullptr;
@@ -544,6 +548,8 @@ cas_status scratch_free(cas_ctx* ctx, Call& c) {
   c.frows = nullptr;
   c.fpos = nullptr;
   c.fstatus = nullptr;
+  c.dbits = nullptr;
+  c.dslot = nullptr;
   return CAS_OK;
 }
 
@@ -685,8 +691,16 @@ cas_status launch_symb_bins(cas_ctx* ctx, Call& c, int64_t* row_nz) {
       case kSB_Dense:
         if (!c.b_sorted && c.ncol > kDenseChunkBits)
           return set_err(ctx, CAS_ERR_BAD_INPUT, "heavy rows over more than %d columns need B rows sorted by column", kDenseChunkBits);
+        if ((double)n * (kRankCols / 8) <= kSavedBitmapBytes) {  // bitmaps kept for the numeric kernel
+          CAS_TRY(dev_alloc(ctx, (void**)&c.dbits, (size_t)n * (kRankCols / 8)));
+          CAS_TRY(dev_alloc(ctx, (void**)&c.dslot, sizeof(int32_t) * (c.m + 1)));
+          CAS_CUDA(ctx, cudaMemsetAsync(c.dslot, 0xFF, sizeof(int32_t) * (c.m + 1), ctx->stream));
+          CAS_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
+          CAS_CUDA(ctx, cudaStreamWaitEvent(s, ctx->ev_fork, 0));
+        }
         k_symb_dense<512><<<(unsigned)n, 512, smem_symb_dense<512>(), s>>>(rows, c.A.csr, c.B.csr, c.ncol,
-                                                                            c.b_sorted ? 1 : 0, row_nz, ctx->d_status);
+                                                                            c.b_sorted ? 1 : 0, row_nz, c.dbits,
+                                                                            c.dslot, ctx->d_status);
         break;
     }
     CAS_TRY(check_launch(ctx, "symbolic bin"));
@@ -778,7 +792,7 @@ cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* 
         if (!c.b_sorted && c.ncol > kRankCols)
           return set_err(ctx, CAS_ERR_BAD_INPUT, "heavy rows over more than %d columns need B rows sorted by column", kRankCols);
         k_numc_dense<512, VIn><<<(unsigned)n, 512, smem_numc_dense<512, VIn>(), s>>>(
-            rows, A, B, c.ncol, c.b_sorted ? 1 : 0, crp, ccol, cval, ctx->d_status);
+            rows, A, B, c.ncol, c.b_sorted ? 1 : 0, crp, ccol, cval, c.dbits, c.dslot, ctx->d_status);
         break;
     }
     CAS_TRY(check_launch(ctx, "numeric bin"));

@@ -383,7 +383,8 @@ __device__ __forceinline__ void row_col_range(const Csr& A, const Csr& B, int64_
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_symb_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int32_t b_sorted,
-             int64_t* __restrict__ row_nz, DevStatus* st) {
+             int64_t* __restrict__ row_nz, uint32_t* __restrict__ saved, int32_t* __restrict__ saved_slot,
+             DevStatus* st) {
   constexpr int W = kDenseChunkBits / 32;
   extern __shared__ __align__(16) uint8_t smem[];
   uint32_t* bm = reinterpret_cast<uint32_t*>(smem);
@@ -408,6 +409,11 @@ k_symb_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int
     if (bad && !multi) dev_report(st, kDevBadIndex, 3, r);
     __syncthreads();
     for (int i = threadIdx.x; i < nw; i += BLOCK) cnt += __popc(bm[i]);
+    if (saved && hi - lo <= kRankCols) {  // one numeric slice: keep the bitmap for the numeric kernel
+      uint32_t* dst = saved + (size_t)blockIdx.x * (kRankCols / 32);
+      for (int i = threadIdx.x; i < nw; i += BLOCK) dst[i] = bm[i];
+      if (threadIdx.x == 0) saved_slot[r] = (int32_t)blockIdx.x;
+    }
     __syncthreads();
   }
   cnt = block_sum<BLOCK, long long>(cnt, sg.tmp);
@@ -1339,13 +1345,12 @@ k_numc_hash(const int32_t* __restrict__ rows, Csr A, Csr B, const int64_t* __res
 // 8 bytes x nnz(row) there).  Shared memory holds 2 bits per column, so four
 // 512-thread blocks fit an SM; a range wider than one slice is cut into
 // slices, B rows cut to each by binary search (B rows sorted).
-constexpr int kRankCols = 1 << 17;  // columns per slice: 16 KiB bitmap + 16 KiB word ranks
 
 template <int BLOCK, typename VIn>
 __global__ void __launch_bounds__(BLOCK)
 k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int32_t b_sorted,
              const int64_t* __restrict__ crp, int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval,
-             DevStatus* st) {
+             const uint32_t* __restrict__ saved, const int32_t* __restrict__ saved_slot, DevStatus* st) {
   using AT = typename Acc<VIn>::T;
   constexpr int NWORD = kRankCols / 32;
   extern __shared__ __align__(16) uint8_t smem[];
@@ -1361,13 +1366,21 @@ k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int
   for (int64_t s0 = lo; s0 < hi; s0 += kRankCols) {
     const int64_t s1 = hi < s0 + kRankCols ? hi : s0 + kRankCols;
     const int nw = (int)((s1 - s0 + 31) >> 5);
-    for (int i = threadIdx.x; i < nw; i += BLOCK) bm[i] = 0u;
-    __syncthreads();
-    expand_row<BLOCK, false, VIn>(A, B, r, sg, multi, (int32_t)s0, (int32_t)s1, [&](int32_t key, VIn, VIn, int64_t) {
-      const int64_t idx = (int64_t)key - s0;
-      if (idx >= 0 && idx < kRankCols) atomicOr(&bm[idx >> 5], 1u << (idx & 31));
-    });
-    __syncthreads();
+    const int32_t slot = (!multi && saved_slot) ? saved_slot[r] : -1;
+    if (slot >= 0) {  // the symbolic kernel kept this row's bitmap
+      const uint32_t* src = saved + (size_t)slot * (kRankCols / 32);
+      for (int i = threadIdx.x; i < nw; i += BLOCK) bm[i] = src[i];
+      __syncthreads();
+    } else {
+      for (int i = threadIdx.x; i < nw; i += BLOCK) bm[i] = 0u;
+      __syncthreads();
+      expand_row<BLOCK, false, VIn>(A, B, r, sg, multi, (int32_t)s0, (int32_t)s1,
+                                    [&](int32_t key, VIn, VIn, int64_t) {
+        const int64_t idx = (int64_t)key - s0;
+        if (idx >= 0 && idx < kRankCols) atomicOr(&bm[idx >> 5], 1u << (idx & 31));
+      });
+      __syncthreads();
+    }
     long long run = 0;
     for (int w0 = 0; w0 < nw; w0 += BLOCK) {
       const int w = w0 + threadIdx.x;
