@@ -929,7 +929,13 @@ __device__ __forceinline__ int warp_sort_compact(uint32_t* __restrict__ skey, AT
 // column of A*A^T alone puts |A_i| products into one bucket.  Shared memory:
 // 13 bytes per product plus half a byte per bucket.
 constexpr int kBucketLimit = 128;
-constexpr int kBigBuckets = 64;  // buckets of more than 8 pairs one row may have
+constexpr int kBigBuckets = 256;  // buckets of more than 8 pairs one row may have
+// Buckets of more than kBucketLimit pairs that span at most kHugeWidth
+// columns (hub columns of a skewed graph, repeated many times) are summed
+// by the whole block into a dense kHugeWidth-slot array over the byte
+// table, which comes out sorted; a row may have kHugeBuckets of them.
+constexpr int kHugeWidth = 256;
+constexpr int kHugeBuckets = 16;
 
 // ---- fused rows: count and place in one pass -------------------------------
 // The fused form of the kernel runs the rows of one product-count range
@@ -1139,7 +1145,8 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
       sum += c0 + c1;
       big = max(big, max(c0, c1));
     }
-    if (__syncthreads_or(big > (uint32_t)kBucketLimit)) {
+    const bool dense_ok = CAP * (int)sizeof(uint8_t) >= kHugeWidth * (int)sizeof(AT) && (1 << shift) <= kHugeWidth;
+    if (__syncthreads_or(big > (uint32_t)kBucketLimit && !dense_ok)) {
       if (FUSED) count_and_defer();
       else if (threadIdx.x == 0) ovf[atomicAdd(ovf_count, 1u)] = (int32_t)r;
       return;
@@ -1179,14 +1186,17 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   // sort each bucket, sum equal columns, compact them to the bucket front:
   // one lane per bucket of at most 8 pairs; larger buckets (about 1 in 100,
   // and the diagonal column's) are queued for a whole warp each
-  __shared__ uint16_t s_big[kBigBuckets];
-  __shared__ int s_nbig;
-  if (threadIdx.x == 0) s_nbig = 0;
+  __shared__ uint16_t s_big[kBigBuckets], s_huge[kHugeBuckets];
+  __shared__ int s_nbig, s_nhuge;
+  if (threadIdx.x == 0) s_nbig = s_nhuge = 0;
   __syncthreads();
   for (int g = warp; g < NG; g += NW) {
     const int b = g * 32 + lane;
     const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
-    if (e - s > 8) {
+    if (e - s > kBucketLimit) {
+      const int slot = atomicAdd(&s_nhuge, 1);
+      if (slot < kHugeBuckets) s_huge[slot] = (uint16_t)b;
+    } else if (e - s > 8) {
       const int slot = atomicAdd(&s_nbig, 1);
       if (slot < kBigBuckets) s_big[slot] = (uint16_t)b;
     } else if (e > s) {
@@ -1194,7 +1204,7 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
     }
   }
   __syncthreads();
-  if (s_nbig > kBigBuckets) {  // uniform: too many large buckets for this form
+  if (s_nbig > kBigBuckets || s_nhuge > kHugeBuckets) {  // uniform: too many large buckets for this form
     if (FUSED) count_and_defer();
     else if (threadIdx.x == 0) ovf[atomicAdd(ovf_count, 1u)] = (int32_t)r;
     return;
@@ -1203,6 +1213,47 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
     const int b = s_big[i];
     const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
     warp_sort_compact<AT>(skey, sval, s, e);
+  }
+  if (s_nhuge > 0) {
+    // the whole block, one huge bucket at a time: sums by column offset in a
+    // dense array over the byte table, then the present columns in order
+    __shared__ uint32_t s_hmask[kHugeWidth / 32];
+    __shared__ int s_hpre[kHugeWidth / 32];
+    AT* dacc = reinterpret_cast<AT*>(segof);
+    const int width = 1 << shift;
+    for (int h = 0; h < s_nhuge; ++h) {
+      const int b = s_huge[h];
+      const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
+      const uint32_t kb = lo + ((uint32_t)b << shift);
+      __syncthreads();
+      for (int j = threadIdx.x; j < width; j += BLOCK) dacc[j] = AT(0);
+      if (threadIdx.x < kHugeWidth / 32) s_hmask[threadIdx.x] = 0u;
+      __syncthreads();
+      for (int i = s + threadIdx.x; i < e; i += BLOCK) {
+        const int off = (int)(skey[i] - kb);
+        atomic_add_sh(&dacc[off], sval[i]);
+        atomicOr(&s_hmask[off >> 5], 1u << (off & 31));
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int run = 0;
+        for (int w = 0; w < kHugeWidth / 32; ++w) {
+          s_hpre[w] = run;
+          run += __popc(s_hmask[w]);
+        }
+      }
+      __syncthreads();
+      const int heads = s_hpre[kHugeWidth / 32 - 1] + __popc(s_hmask[kHugeWidth / 32 - 1]);
+      for (int j = threadIdx.x; j < width; j += BLOCK) {
+        const uint32_t m = s_hmask[j >> 5];
+        if (m & (1u << (j & 31))) {
+          const int pos = s + s_hpre[j >> 5] + __popc(m & ((1u << (j & 31)) - 1u));
+          skey[pos] = kb + (uint32_t)j;
+          sval[pos] = dacc[j];
+        }
+      }
+      for (int i = s + heads + threadIdx.x; i < e; i += BLOCK) skey[i] = kEmptyKey;
+    }
   }
   __syncthreads();
   // distinct pairs per 32-slot chunk, then chunk offsets

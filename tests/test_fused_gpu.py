@@ -22,9 +22,9 @@ def same(out, ref):
     np.testing.assert_array_equal(out.csr.vals.astype(np.float64), ref[2])
 
 
-def hot_column_matrix(seed=3):
+def hot_column_matrix(seed=3, ncol=3000):
     """Rows whose products crowd one bucket: 160 A entries whose B rows all
-    hold column 0 (so 160 equal keys), plus a narrow band of distinct columns."""
+    hold column 0 (so 160 equal keys), plus other columns below ncol."""
     rng = np.random.default_rng(seed)
     n_rows, n_mid = 40, 400
     r, c = [], []
@@ -35,10 +35,10 @@ def hot_column_matrix(seed=3):
     A = from_coo(n_rows, n_mid, np.array(r), np.array(c))
     br, bc = [], []
     for k in range(n_mid):
-        cols = np.concatenate([[0], rng.choice(np.arange(1, 3000), 19, replace=False)])
+        cols = np.concatenate([[0], rng.choice(np.arange(1, ncol), 19, replace=False)])
         br += [k] * 20
         bc += list(cols)
-    B = from_coo(n_mid, 3000, np.array(br), np.array(bc))
+    B = from_coo(n_mid, ncol, np.array(br), np.array(bc))
     return A, B
 
 
@@ -60,11 +60,28 @@ def test_er_rows_fused(ctx, algo):
 
 
 def test_overflowing_fused_rows_are_deferred(ctx):
-    A, B = hot_column_matrix()
+    # columns spread over 4M: the hot column's bucket spans 2048 columns, too
+    # wide to sum densely, so each row is counted in-kernel and deferred
+    A, B = hot_column_matrix(ncol=1 << 22)
     ref = oracle.oracle_spgemm(A, B, "hybacc")
     out = ctx.spgemm(A, B, "hybacc")
     assert out.stats["fused_rows"] == A.num_row
     assert out.stats["esc_overflow_rows"] == A.num_row
+    same(out, ref)
+
+
+@pytest.mark.parametrize("fuse", [True, False])
+def test_huge_narrow_buckets_summed_densely(ctx, fuse):
+    # columns below 3000: the hot column's bucket spans 2 columns, summed by
+    # the whole block in place, no row deferred
+    A, B = hot_column_matrix()
+    ref = oracle.oracle_spgemm(A, B, "hybacc")
+    ctx.set_fusion(fuse)
+    try:
+        out = ctx.spgemm(A, B, "hybacc")
+    finally:
+        ctx.set_fusion(True)
+    assert out.stats["esc_overflow_rows"] == 0
     same(out, ref)
 
 
