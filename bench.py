@@ -37,10 +37,13 @@ sys.path.insert(0, os.path.join(ROOT, "contention-aware-spgemm_b200"))
 import numpy as np  # noqa: E402
 
 WORKLOADS = {
-    # name: (family, scale, edge_factor, seed)
+    # name: (family, scale, edge_factor, seed) for R-MAT; the Zipf bipartite
+    # join-aggregate stand-in: 850,000 x 2,000,000, 12 M nonzeros, row degrees
+    # Zipf(1.2) up to 50,000, column popularity Zipf(1.4) shifted by q_c = 1000
     "er_s21_ef32": ("er", 21, 32, 21),
     "g500_s17_ef8": ("g500", 17, 8, 17),
     "er_s18_ef32": ("er", 18, 32, 18),
+    "zipf_850k": ("zipf", 850000, 2000000, 3),
 }
 
 
@@ -49,10 +52,15 @@ def log(*a):
 
 
 def make_matrix(name):
+    """(A, B = A^T): the same CSR for the symmetric R-MAT graphs, the explicit
+    transpose for the Zipf bipartite matrix."""
     import casgemm
     fam, s, ef, seed = WORKLOADS[name]
+    if fam == "zipf":
+        A = casgemm.gen_zipf(s, ef, 50000, 12000000, seed, col_q=1000.0)
+        return A, A.transpose()
     A = casgemm.gen_er(s, ef, seed) if fam == "er" else casgemm.gen_g500(s, ef, seed)
-    return A
+    return A, A
 
 
 def row_products(A, B):
@@ -191,8 +199,7 @@ def total_products(A, B):
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
-    A = make_matrix(args.workload)
-    B = A  # symmetric: Aᵀ has the same CSR
+    A, B = make_matrix(args.workload)
     base = cpu_reference(A, B, args.ref_products, args.steps, args.warmup)
     line = {"metric": "SpGEMM GFLOP/s (2 x intermediate products / s), C = A*A^T",
             "value": base["value"], "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -422,8 +429,7 @@ def main():
     dev = torch.device("cuda", torch.cuda.current_device())
 
     t0 = time.time()
-    A = make_matrix(args.workload)
-    B = A  # Aᵀ of a symmetric matrix has the same CSR
+    A, B = make_matrix(args.workload)
     r_end = max(1, int(round(A.num_row * args.row_fraction)))
     r0, r1 = row_shard(A, B, rank, world, r_end)
     As = slice_rows(A, r0, r1)
@@ -527,7 +533,7 @@ def main():
         "data": "synthetic (seeded R-MAT, values 1.0)",
         "config": {"workload": args.workload, "accumulator": args.accum, "row_fraction": args.row_fraction,
                    "products": P_total, "nnz_c": nnz_total, "nnz_a": A.nnz, "n": A.num_row,
-                   "l2": "not flushed: inputs (1.6 GB each) exceed the 126 MB L2",
+                   "l2": f"not flushed: inputs ({12 * A.nnz / 1e9:.2f} GB each) exceed the 126 MB L2",
                    "parallelism": f"row shards x{world}" if world > 1 else "1 GPU",
                    "phases_ms_last_step": {k: round(v * 1e3, 3) for k, v in rts[-1].items()}},
         "roofline": {"bound": "hbm", "kernel": kernel_name, "bin": dom,
@@ -549,7 +555,7 @@ def main():
     if not args.no_e2e:
         pin = lambda x: torch.from_numpy(np.ascontiguousarray(x)).pin_memory()  # noqa: E731
         hA = [pin(As.row_ptrs), pin(As.cols), pin(As.vals)]
-        hB = hA if (world == 1) else [pin(B.row_ptrs), pin(B.cols), pin(B.vals)]
+        hB = hA if (world == 1 and B is A) else [pin(B.row_ptrs), pin(B.cols), pin(B.vals)]
         ca = casgemm.CasCsr(As.num_row, As.num_col, As.nnz, hA[0].data_ptr(), hA[1].data_ptr(), hA[2].data_ptr(),
                             4, 0, 0, 0)
         cb = casgemm.CasCsr(B.num_row, B.num_col, B.nnz, hB[0].data_ptr(), hB[1].data_ptr(), hB[2].data_ptr(),

@@ -165,7 +165,8 @@ constexpr size_t smem_numc_hash() {
 }
 template <int BLOCK, typename VIn>
 constexpr size_t smem_numc_dense() {
-  return size_t(cas::kRankCols / 32) * 8 + sizeof(cas::Stage<VIn>);
+  return size_t(cas::kRankCols / 32) * 4 + size_t(cas::kRankCols / 256) * 4 + size_t(cas::kRankCols / 32) * 2 +
+         sizeof(cas::Stage<VIn>);
 }
 
 template <int CAP, int NBB, typename VIn>

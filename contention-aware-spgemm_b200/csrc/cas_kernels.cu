@@ -1389,14 +1389,14 @@ k_numc_hash(const int32_t* __restrict__ rows, Csr A, Csr B, const int64_t* __res
 
 // Heavy rows in one pass per slice of kRankCols columns of the row's column
 // range: a keys-only expansion marks the row's columns in a shared-memory
-// bitmap, an exclusive scan of the words' population counts ranks every
-// column, the column indices are written to C from the bitmap and the values
-// zeroed, and a second expansion adds every product straight into its place
-// in C with a global atomic add (resolved in L2: a row's values are at most
-// 8 bytes x nnz(row) there).  Shared memory holds 2 bits per column, so four
-// 512-thread blocks fit an SM; a range wider than one slice is cut into
-// slices, B rows cut to each by binary search (B rows sorted).
-
+// bitmap (or the symbolic kernel's kept bitmap is loaded), the rank of every
+// column comes from a 32-bit base per group of 8 words plus a 16-bit rank of
+// each word within its group, the column indices are written to C from the
+// bitmap and the values zeroed, and a second expansion adds every product
+// straight into its place in C with a global atomic add (resolved in L2: a
+// row's values are at most 8 bytes x nnz(row) there).  A range wider than one
+// slice is cut into slices, B rows cut to each by binary search (B rows
+// sorted).
 template <int BLOCK, typename VIn>
 __global__ void __launch_bounds__(BLOCK)
 k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int32_t b_sorted,
@@ -1406,8 +1406,9 @@ k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int
   constexpr int NWORD = kRankCols / 32;
   extern __shared__ __align__(16) uint8_t smem[];
   uint32_t* bm = reinterpret_cast<uint32_t*>(smem);
-  uint32_t* rank = bm + NWORD;
-  Stage<VIn>& sg = *reinterpret_cast<Stage<VIn>*>(reinterpret_cast<uint8_t*>(rank + NWORD));
+  uint32_t* gbase = bm + NWORD;                                       // NWORD / 8 group bases
+  uint16_t* wrank = reinterpret_cast<uint16_t*>(gbase + NWORD / 8);   // NWORD ranks within the group
+  Stage<VIn>& sg = *reinterpret_cast<Stage<VIn>*>(reinterpret_cast<uint8_t*>(wrank + NWORD));
   const int64_t r = rows[blockIdx.x];
   const int64_t c0r = crp[r], nz = crp[r + 1] - c0r;
   int64_t lo, hi;
@@ -1432,12 +1433,22 @@ k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int
       });
       __syncthreads();
     }
+    const int ng = (nw + 7) >> 3;
     long long run = 0;
-    for (int w0 = 0; w0 < nw; w0 += BLOCK) {
-      const int w = w0 + threadIdx.x;
+    for (int g0 = 0; g0 < ng; g0 += BLOCK) {
+      const int g = g0 + threadIdx.x;
+      int cnt = 0;
+      if (g < ng) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int w = g * 8 + k;
+          wrank[w] = (uint16_t)cnt;
+          cnt += w < nw ? __popc(bm[w]) : 0;
+        }
+      }
       long long tot;
-      const long long ex = block_exclusive_sum<BLOCK, long long>(w < nw ? (long long)__popc(bm[w]) : 0ll, sg.tmp, tot);
-      if (w < nw) rank[w] = (uint32_t)(run + ex);
+      const long long ex = block_exclusive_sum<BLOCK, long long>((long long)cnt, sg.tmp, tot);
+      if (g < ng) gbase[g] = (uint32_t)(run + ex);
       run += tot;
     }
     __syncthreads();
@@ -1445,7 +1456,7 @@ k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int
     const int64_t room = nz - written;  // guards the writes if the counts disagree
     for (int w = threadIdx.x; w < nw; w += BLOCK) {
       uint32_t word = bm[w];
-      int64_t pos = rank[w];
+      int64_t pos = (int64_t)gbase[w >> 3] + wrank[w];
       while (word) {
         const int b = __ffs(word) - 1;
         word &= word - 1;
@@ -1462,7 +1473,7 @@ k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int
       const int64_t idx = (int64_t)key - s0;
       if (idx < 0 || idx >= kRankCols) return;
       const int w = (int)(idx >> 5);
-      const int64_t pos = rank[w] + __popc(bm[w] & ((1u << (idx & 31)) - 1u));
+      const int64_t pos = (int64_t)gbase[w >> 3] + wrank[w] + __popc(bm[w] & ((1u << (idx & 31)) - 1u));
       if (pos < room) Acc<VIn>::atomic_add(&cval[base + pos], Acc<VIn>::mul(av, bv));
     });
     written += run;

@@ -60,8 +60,8 @@ enum NumcBin : int {
 
 enum AccumMode : int { kAccHash = 0, kAccEsc = 1, kAccHybrid = 2 };
 
-constexpr int kDenseChunkBits = 1 << 18;   // symbolic bitmap slice: 256 Ki columns (32 KiB)
-constexpr int kRankCols = 1 << 17;         // numeric dense slice: 128 Ki columns (16 KiB bitmap + 16 KiB ranks)
+constexpr int kDenseChunkBits = 1 << 19;   // symbolic bitmap slice: 512 Ki columns (64 KiB)
+constexpr int kRankCols = 1 << 19;         // numeric dense slice: 512 Ki columns (64 + 32 + 8 KiB of bitmap and ranks)
 
 struct Csr {
   int64_t nrow, ncol;
