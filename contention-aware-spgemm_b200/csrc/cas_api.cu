@@ -33,7 +33,7 @@
 namespace {
 
 constexpr int kAux = 4;          // auxiliary streams for concurrent bins
-constexpr int kCountSlots = 128; // device/pinned counter block
+constexpr int kCountSlots = 256; // device/pinned counter block
 
 // Layout of the counter block (unsigned long long slots).
 constexpr int kSlotSymb = 0;     // [0, 9)   symbolic bin counts
@@ -45,6 +45,8 @@ constexpr int kSlotCheck = 48;   // [48, 52) input check flags
 constexpr int kSlotBinSums = 64; // [64, 103) per numeric bin: products, nnz(C), nnz(A)
 constexpr int kSlotOvf = 110;    // [110]   rows handed to the radix-sort ESC kernel
 constexpr int kSlotFused = 112;  // [112, 116) fused rows: count, products, output bound, nnz(A); [116] ticket
+constexpr int kSlotHeavy = 128;  // [128, 176) dense rows per size class
+constexpr int kSlotHeavyCur = 176;  // [176, 224) their cursors
 constexpr size_t kStageBytes = size_t(64) << 20;  // pinned staging chunk for host copies
 constexpr double kSavedBitmapBytes = 8.0 * (1ull << 30);  // heavy-row bitmaps kept between the phases
 
@@ -717,29 +719,44 @@ cas_status numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int mode) {
   CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + kSlotNumc, 0, sizeof(unsigned long long) * kNumcBins, ctx->stream));
   CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + kSlotBinSums, 0, sizeof(unsigned long long) * 3 * kNumcBins,
                                 ctx->stream));
+  CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + kSlotHeavy, 0, sizeof(unsigned long long) * kHeavyClasses,
+                                ctx->stream));
   if (c.m > 0) {
     k_bin_count_numc<<<grid_for(c.m, 256, ctx->sm_count * 8), 256, 0, ctx->stream>>>(
         c.m, c.row_flp, crp, c.A.csr.rp, mode, ctx->acc_thres, ctx->d_counts + kSlotNumc,
-        ctx->d_counts + kSlotBinSums);
+        ctx->d_counts + kSlotBinSums, ctx->d_counts + kSlotHeavy);
     CAS_TRY(check_launch(ctx, "k_bin_count_numc"));
   }
   CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotNumc, ctx->d_counts + kSlotNumc,
                                 sizeof(unsigned long long) * kNumcBins, cudaMemcpyDeviceToHost, ctx->stream));
   CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotBinSums, ctx->d_counts + kSlotBinSums,
                                 sizeof(unsigned long long) * 3 * kNumcBins, cudaMemcpyDeviceToHost, ctx->stream));
+  CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotHeavy, ctx->d_counts + kSlotHeavy,
+                                sizeof(unsigned long long) * kHeavyClasses, cudaMemcpyDeviceToHost, ctx->stream));
   CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   unsigned long long* cur = ctx->h_counts + kSlotCursor;
   unsigned long long off = 0;
   for (int b = 0; b < kNumcBins; ++b) {
     c.numc_count[b] = (int64_t)ctx->h_counts[kSlotNumc + b];
     cur[b] = off;
+    if (b == kNB_Dense) {  // heaviest size class first
+      unsigned long long* hc = ctx->h_counts + kSlotHeavyCur;
+      unsigned long long o = off;
+      for (int k = 0; k < kHeavyClasses; ++k) {
+        hc[k] = o;
+        o += ctx->h_counts[kSlotHeavy + k];
+      }
+    }
     off += ctx->h_counts[kSlotNumc + b];
   }
   if (c.m > 0) {
     CAS_CUDA(ctx, cudaMemcpyAsync(ctx->d_counts + kSlotCursor, cur, sizeof(unsigned long long) * kNumcBins,
                                   cudaMemcpyHostToDevice, ctx->stream));
+    CAS_CUDA(ctx, cudaMemcpyAsync(ctx->d_counts + kSlotHeavyCur, ctx->h_counts + kSlotHeavyCur,
+                                  sizeof(unsigned long long) * kHeavyClasses, cudaMemcpyHostToDevice, ctx->stream));
     k_bin_scatter_numc<<<grid_for(c.m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
-        c.m, c.row_flp, crp, mode, ctx->acc_thres, ctx->d_counts + kSlotCursor, c.rows);
+        c.m, c.row_flp, crp, mode, ctx->acc_thres, ctx->d_counts + kSlotCursor, ctx->d_counts + kSlotHeavyCur,
+        c.rows);
     CAS_TRY(check_launch(ctx, "k_bin_scatter_numc"));
   }
   return CAS_OK;

@@ -87,15 +87,28 @@ __global__ void k_fused_scatter(int64_t m, const int64_t* __restrict__ row_flp, 
 
 // Numeric bin histogram plus, per bin, the sums of products, nnz(C) and
 // nnz(A) of its rows (for the per-kernel algorithmic byte count).
+// Heavy rows launch heaviest first (longest-processing-time order, so the
+// largest rows do not start last and run alone): within the dense bin, rows
+// are grouped by floor(log2(products)), the largest group first.
+constexpr int kHeavyClasses = 48;
+__device__ __forceinline__ int heavy_class(int64_t flp) {  // 0 for the heaviest rows
+  const int l = 63 - __clzll((unsigned long long)flp);
+  return l >= kHeavyClasses ? 0 : kHeavyClasses - 1 - l;
+}
+
 __global__ void k_bin_count_numc(int64_t m, const int64_t* __restrict__ row_flp, const int64_t* __restrict__ crp,
                                  const int64_t* __restrict__ arp, int mode, double thres,
-                                 unsigned long long* __restrict__ bin_count, unsigned long long* __restrict__ bin_sums) {
+                                 unsigned long long* __restrict__ bin_count, unsigned long long* __restrict__ bin_sums,
+                                 unsigned long long* __restrict__ heavy_count) {
   __shared__ unsigned long long s_cnt[4 * kNumcBins];
+  __shared__ unsigned long long s_heavy[kHeavyClasses];
   if (threadIdx.x < 4 * kNumcBins) s_cnt[threadIdx.x] = 0;
+  if (threadIdx.x < kHeavyClasses) s_heavy[threadIdx.x] = 0;
   __syncthreads();
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
     const int64_t flp = row_flp[r], nz = crp[r + 1] - crp[r];
     const int b = numc_bin_of(flp, nz, mode, thres);
+    if (b == kNB_Dense) atomicAdd(&s_heavy[heavy_class(flp)], 1ull);
     atomicAdd(&s_cnt[b], 1ull);
     atomicAdd(&s_cnt[kNumcBins + b], (unsigned long long)flp);
     atomicAdd(&s_cnt[2 * kNumcBins + b], (unsigned long long)nz);
@@ -105,14 +118,17 @@ __global__ void k_bin_count_numc(int64_t m, const int64_t* __restrict__ row_flp,
   if (threadIdx.x < kNumcBins && s_cnt[threadIdx.x]) atomicAdd(&bin_count[threadIdx.x], s_cnt[threadIdx.x]);
   if (threadIdx.x >= kNumcBins && threadIdx.x < 4 * kNumcBins && s_cnt[threadIdx.x])
     atomicAdd(&bin_sums[threadIdx.x - kNumcBins], s_cnt[threadIdx.x]);
+  if (threadIdx.x < kHeavyClasses && s_heavy[threadIdx.x]) atomicAdd(&heavy_count[threadIdx.x], s_heavy[threadIdx.x]);
 }
 
 __global__ void k_bin_scatter_numc(int64_t m, const int64_t* __restrict__ row_flp, const int64_t* __restrict__ crp,
                                    int mode, double thres, unsigned long long* __restrict__ cursor,
-                                   int32_t* __restrict__ rows) {
+                                   unsigned long long* __restrict__ heavy_cursor, int32_t* __restrict__ rows) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
-    const int b = numc_bin_of(row_flp[r], crp[r + 1] - crp[r], mode, thres);
-    const unsigned long long pos = warp_aggregated_add(cursor, b);
+    const int64_t flp = row_flp[r];
+    const int b = numc_bin_of(flp, crp[r + 1] - crp[r], mode, thres);
+    const unsigned long long pos =
+        b == kNB_Dense ? warp_aggregated_add(heavy_cursor, heavy_class(flp)) : warp_aggregated_add(cursor, b);
     rows[pos] = (int32_t)r;
   }
 }
