@@ -743,6 +743,22 @@ __device__ __forceinline__ void sort8(uint32_t (&k)[8], uint32_t (&p)[8]) {
   cswap(k[1], p[1], k[2], p[2]); cswap(k[3], p[3], k[4], p[4]);
   cswap(k[5], p[5], k[6], p[6]);
 }
+// Optimal networks for 4 (5 comparators) and 6 inputs (12 comparators), for
+// warps whose buckets are all small; all three are checked exhaustively on
+// 0/1 inputs by the 0-1 principle.
+__device__ __forceinline__ void sort_net(uint32_t (&k)[4], uint32_t (&p)[4]) {
+  cswap(k[0], p[0], k[1], p[1]); cswap(k[2], p[2], k[3], p[3]);
+  cswap(k[0], p[0], k[2], p[2]); cswap(k[1], p[1], k[3], p[3]);
+  cswap(k[1], p[1], k[2], p[2]);
+}
+__device__ __forceinline__ void sort_net(uint32_t (&k)[6], uint32_t (&p)[6]) {
+  cswap(k[0], p[0], k[5], p[5]); cswap(k[1], p[1], k[3], p[3]); cswap(k[2], p[2], k[4], p[4]);
+  cswap(k[1], p[1], k[2], p[2]); cswap(k[3], p[3], k[4], p[4]);
+  cswap(k[0], p[0], k[3], p[3]); cswap(k[2], p[2], k[5], p[5]);
+  cswap(k[0], p[0], k[1], p[1]); cswap(k[2], p[2], k[3], p[3]); cswap(k[4], p[4], k[5], p[5]);
+  cswap(k[1], p[1], k[2], p[2]); cswap(k[3], p[3], k[4], p[4]);
+}
+__device__ __forceinline__ void sort_net(uint32_t (&k)[8], uint32_t (&p)[8]) { sort8(k, p); }
 
 // Products of a staged chunk too large for the byte table: the A entry of
 // product p is found by binary search over the 32-bit prefixes.
@@ -822,28 +838,29 @@ __device__ __forceinline__ void atomic_add_sh(long long* p, long long v) {
   atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
 }
 
-// Sorts the (key, value) pairs of one bucket [s, e), 1 <= e - s <= 8, in
-// shared memory by key with the 8-input network in registers, sums equal
+// Sorts the (key, value) pairs of one bucket [s, e), 1 <= e - s <= N, in
+// shared memory by key with the N-input network in registers, sums equal
 // keys, and leaves the distinct (key, sum) pairs at [s, s + heads) and
-// kEmptyKey behind them; returns heads.  One lane per bucket.
-template <typename AT>
+// kEmptyKey behind them; returns heads.  One lane per bucket; the caller
+// picks N from the largest bucket of the warp.
+template <int N, typename AT>
 __device__ __forceinline__ int sort_compact_small(uint32_t* __restrict__ skey, AT* __restrict__ sval, int s, int e) {
   const int nb = e - s;
-  uint32_t k[8], q[8];
+  uint32_t k[N], q[N];
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
+  for (int i = 0; i < N; ++i) {
     k[i] = i < nb ? skey[s + i] : 0xFFFFFFFFu;
     q[i] = (uint32_t)i;
   }
-  sort8(k, q);
-  AT v[8];
+  sort_net(k, q);
+  AT v[N];
 #pragma unroll
-  for (int i = 0; i < 8; ++i) v[i] = i < nb ? sval[s + q[i]] : AT(0);
+  for (int i = 0; i < N; ++i) v[i] = i < nb ? sval[s + q[i]] : AT(0);
   int h = 0;
   uint32_t prev = k[0];
   AT acc = v[0];
 #pragma unroll
-  for (int i = 1; i < 8; ++i) {
+  for (int i = 1; i < N; ++i) {
     if (i < nb) {
       if (k[i] != prev) {
         skey[s + h] = prev;
@@ -863,10 +880,6 @@ __device__ __forceinline__ int sort_compact_small(uint32_t* __restrict__ skey, A
   return h;
 }
 
-// The same for a bucket of 8 < e - s <= 128 pairs, by a whole warp: every
-// pair's rank is counted against the bucket read by broadcast, the pairs are
-// written back in key order, equal keys are summed into their run's first
-// slot with shared-memory atomics, and the tail is marked kEmptyKey.
 template <typename AT>
 __device__ __forceinline__ int warp_sort_compact(uint32_t* __restrict__ skey, AT* __restrict__ sval, int s, int e) {
   constexpr int PER = 4;
@@ -1215,8 +1228,15 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
     } else if (e - s > 8) {
       const int slot = atomicAdd(&s_nbig, 1);
       if (slot < kBigBuckets) s_big[slot] = (uint16_t)b;
-    } else if (e > s) {
-      sort_compact_small<AT>(skey, sval, s, e);
+    }
+    // one network size for the whole warp: the smallest that fits its
+    // largest bucket of at most 8 pairs
+    const int small = (e - s <= 8) ? e - s : 0;
+    const int mx = __reduce_max_sync(kFull, small);
+    if (small > 0) {
+      if (mx <= 4) sort_compact_small<4, AT>(skey, sval, s, e);
+      else if (mx <= 6) sort_compact_small<6, AT>(skey, sval, s, e);
+      else sort_compact_small<8, AT>(skey, sval, s, e);
     }
   }
   __syncthreads();
