@@ -402,6 +402,8 @@ def main():
                     help="products in the CPU reference's row sample")
     ap.add_argument("--row-fraction", type=float, default=1.0,
                     help="use only the first fraction of A's rows (profiling captures; B stays whole)")
+    ap.add_argument("--tune", default=None, metavar="CACHE.json",
+                    help="pick the row routing with casgemm.Autotuner (cached in CACHE.json) before timing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -446,6 +448,14 @@ def main():
     ctx = casgemm.Context(dev.index)
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
+
+    tuning = None
+    if args.tune:
+        tuner = casgemm.Autotuner(ctx, args.tune)
+        key = casgemm.Autotuner.key(As, B)
+        tuning = dict(tuner.tune(key, dA, dB, args.accum), key=key)
+        tuner.apply(key)
+        log(f"[rank {rank}] tuning {tuning}")
 
     def step():
         cc, rt = ctx.spgemm_device(dA, dB, args.accum)
@@ -535,7 +545,8 @@ def main():
                    "products": P_total, "nnz_c": nnz_total, "nnz_a": A.nnz, "n": A.num_row,
                    "l2": f"not flushed: inputs ({12 * A.nnz / 1e9:.2f} GB each) exceed the 126 MB L2",
                    "parallelism": f"row shards x{world}" if world > 1 else "1 GPU",
-                   "phases_ms_last_step": {k: round(v * 1e3, 3) for k, v in rts[-1].items()}},
+                   "phases_ms_last_step": {k: round(v * 1e3, 3) for k, v in rts[-1].items()},
+                   "tuning": tuning if tuning else ctx.get_tuning()},
         "roofline": {"bound": "hbm", "kernel": kernel_name, "bin": dom,
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": peak_kind,

@@ -104,6 +104,16 @@ class CasServerStats(ctypes.Structure):
     ]
 
 
+class CasTuning(ctypes.Structure):
+    _fields_ = [
+        ("acc_thres", ctypes.c_double), ("fusion", ctypes.c_int32), ("fused_min_products", ctypes.c_int32),
+        ("esc_max_products", ctypes.c_int32), ("hash_max_nnz", ctypes.c_int32),
+    ]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class CasError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"{STATUS.get(status, status)}: {msg}")
@@ -130,6 +140,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "cas_last_error": (ctypes.c_char_p, [P]),
         "cas_set_profiling": (I32, [P, ctypes.c_int]),
         "cas_set_fusion": (I32, [P, ctypes.c_int]),
+        "cas_set_tuning": (I32, [P, ctypes.POINTER(CasTuning)]),
+        "cas_get_tuning": (I32, [P, ctypes.POINTER(CasTuning)]),
         "cas_get_stats": (I32, [P, ctypes.POINTER(CasStats)]),
         "cas_spgemm": (I32, [P, I32, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr),
                              ctypes.POINTER(CasRuntime)]),
@@ -255,6 +267,22 @@ class Context:
 
     def set_acc_thres(self, thres: float):
         self._check(self.lib.cas_set_acc_thres(self.h, float(thres)))
+
+    def get_tuning(self) -> dict:
+        t = CasTuning()
+        self._check(self.lib.cas_get_tuning(self.h, ctypes.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        """Change the routing of rows to kernels (cas_set_tuning); unnamed knobs keep their values."""
+        cur = self.get_tuning()
+        unknown = set(kw) - set(cur)
+        if unknown:
+            raise ValueError(f"unknown tuning knobs {sorted(unknown)}")
+        cur.update(kw)
+        t = CasTuning(float(cur["acc_thres"]), int(cur["fusion"]), int(cur["fused_min_products"]),
+                      int(cur["esc_max_products"]), int(cur["hash_max_nnz"]))
+        self._check(self.lib.cas_set_tuning(self.h, ctypes.byref(t)))
 
     def set_fusion(self, on: bool):
         self._check(self.lib.cas_set_fusion(self.h, int(bool(on))))
@@ -440,6 +468,80 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+
+class Autotuner:
+    """Picks the routing of rows to kernels (cas_tuning) per class of input.
+
+    The class is a key from the degree distribution of the product: log2 of
+    the mean products per row (rounded), log2 of the largest row's products
+    over the mean (the skew, rounded down), log2 of the column count, and the
+    value type.  For a
+    class not yet in the cache, `tune` times every candidate setting on the
+    given device matrices (best of `trials` runs by the pipeline's own CUDA
+    events) and keeps the fastest; the cache is a JSON file, so a class is
+    tuned once.  Every candidate computes the same C; only the speed differs.
+    """
+
+    CANDIDATES = ([{"acc_thres": a, "fusion": 1, "fused_min_products": lo, "esc_max_products": e,
+                    "hash_max_nnz": 4096}
+                   for a in (1.5, 2.0, 5.0) for lo in (1024, 2048, 3072) for e in (4096, 8192)]
+                  + [{"acc_thres": 2.0, "fusion": 0, "fused_min_products": 2048, "esc_max_products": 8192,
+                      "hash_max_nnz": 4096}])
+
+    def __init__(self, ctx: "Context", cache_path: Optional[str] = None):
+        self.ctx = ctx
+        self.path = cache_path
+        self.cache = {}
+        if cache_path and os.path.exists(cache_path):
+            import json
+            with open(cache_path) as fh:
+                self.cache = json.load(fh)
+
+    @staticmethod
+    def key(A: Csr, B: Csr) -> str:
+        import math
+        rows = np.diff(row_products_prefix(A, B))
+        mean = float(rows.mean()) if len(rows) else 0.0
+        mx = float(rows.max()) if len(rows) else 0.0
+        lg = lambda x: int(round(math.log2(x))) if x > 0 else 0  # noqa: E731
+        skew = int(math.floor(math.log2(mx / mean))) if mean > 0 and mx > 0 else 0
+        vt = "i32" if A.vals.dtype == np.int32 else "f64"
+        return f"p{lg(mean)}_s{skew}_c{lg(B.num_col)}_{vt}"
+
+    def tune(self, key: str, dA: "DeviceCsr", dB: "DeviceCsr", accum: str = "hybacc", trials: int = 2) -> dict:
+        if key in self.cache:
+            return self.cache[key]
+        saved = self.ctx.get_tuning()
+        timed = []
+        try:
+            for cand in self.CANDIDATES:
+                self.ctx.set_tuning(**cand)
+                best = float("inf")
+                for _ in range(trials):
+                    cc, rt = self.ctx.spgemm_device(dA, dB, accum)
+                    self.ctx.free(cc)
+                    best = min(best, rt["total_time"])
+                timed.append((best, cand))
+        finally:
+            self.ctx.set_tuning(**saved)
+        best_t, best = min(timed, key=lambda x: x[0])
+        default_t = next((t for t, c in timed if c == saved), None)  # the setting the context had
+        self.cache[key] = dict(best, seconds=best_t, default_seconds=default_t)
+        if self.path:
+            import json
+            with open(self.path, "w") as fh:
+                json.dump(self.cache, fh, indent=1, sort_keys=True)
+        return self.cache[key]
+
+    def apply(self, key: str) -> bool:
+        """Sets the cached choice for `key` on the context; False if the class was never tuned."""
+        cfg = self.cache.get(key)
+        if not cfg:
+            return False
+        self.ctx.set_tuning(**{k: cfg[k] for k in ("acc_thres", "fusion", "fused_min_products",
+                                                    "esc_max_products", "hash_max_nnz")})
+        return True
 
 
 # ---------------------------------------------------------------- data layer

@@ -66,6 +66,9 @@ struct cas_ctx {
   cudaEvent_t ev_ovf[2] = {};
   bool profile = false;
   bool fuse = true;                        // fused ESC rows (no symbolic pass) in cas_spgemm
+  int fused_lo = (int)cas::kFusedLo;       // fused rows: more products than this (up to kFusedHi)
+  int esc_max = 8192;                      // ESC rows: at most this many products
+  int hash_max = 4096;                     // hash rows: at most this many distinct columns
   double acc_thres = 2.0;
   cudaEvent_t ev_fused[2] = {};
   std::string err;
@@ -723,8 +726,8 @@ cas_status numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int mode) {
                                 ctx->stream));
   if (c.m > 0) {
     k_bin_count_numc<<<grid_for(c.m, 256, ctx->sm_count * 8), 256, 0, ctx->stream>>>(
-        c.m, c.row_flp, crp, c.A.csr.rp, mode, ctx->acc_thres, ctx->d_counts + kSlotNumc,
-        ctx->d_counts + kSlotBinSums, ctx->d_counts + kSlotHeavy);
+        c.m, c.row_flp, crp, c.A.csr.rp, mode, ctx->acc_thres, ctx->esc_max, ctx->hash_max,
+        ctx->d_counts + kSlotNumc, ctx->d_counts + kSlotBinSums, ctx->d_counts + kSlotHeavy);
     CAS_TRY(check_launch(ctx, "k_bin_count_numc"));
   }
   CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotNumc, ctx->d_counts + kSlotNumc,
@@ -755,8 +758,8 @@ cas_status numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int mode) {
     CAS_CUDA(ctx, cudaMemcpyAsync(ctx->d_counts + kSlotHeavyCur, ctx->h_counts + kSlotHeavyCur,
                                   sizeof(unsigned long long) * kHeavyClasses, cudaMemcpyHostToDevice, ctx->stream));
     k_bin_scatter_numc<<<grid_for(c.m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
-        c.m, c.row_flp, crp, mode, ctx->acc_thres, ctx->d_counts + kSlotCursor, ctx->d_counts + kSlotHeavyCur,
-        c.rows);
+        c.m, c.row_flp, crp, mode, ctx->acc_thres, ctx->esc_max, ctx->hash_max, ctx->d_counts + kSlotCursor,
+        ctx->d_counts + kSlotHeavyCur, c.rows);
     CAS_TRY(check_launch(ctx, "k_bin_scatter_numc"));
   }
   return CAS_OK;
@@ -861,7 +864,7 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
   const int c_col_bytes = c_on_device ? 4 : (C->col_bytes == 8 ? 8 : 4);
   CAS_TRY(prepare(ctx, A, B, c, h2d));
   memset(C, 0, sizeof(*C));
-  c.fuse = ctx->fuse && accum != CAS_ACC_HASH ? 1 : 0;
+  c.fuse = ctx->fuse && accum != CAS_ACC_HASH ? ctx->fused_lo : 0;
   const size_t vbytes = 8;  // fp64 or int64 output
   CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[0], ctx->stream));
   // INIT
@@ -1120,6 +1123,29 @@ cas_status cas_set_acc_thres(cas_ctx* ctx, double thres) {
 }
 
 const char* cas_last_error(const cas_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+cas_status cas_set_tuning(cas_ctx* ctx, const cas_tuning* t) {
+  if (!ctx || !t) return CAS_ERR_BAD_INPUT;
+  if (!(t->acc_thres >= 0.0) || t->fused_min_products < 32 || t->fused_min_products >= (int)cas::kFusedHi ||
+      t->esc_max_products < 32 || t->esc_max_products > 8192 || t->hash_max_nnz < 0 || t->hash_max_nnz > 4096)
+    return set_err(ctx, CAS_ERR_BAD_INPUT, "tuning out of range");
+  ctx->acc_thres = t->acc_thres;
+  ctx->fuse = t->fusion != 0;
+  ctx->fused_lo = t->fused_min_products;
+  ctx->esc_max = t->esc_max_products;
+  ctx->hash_max = t->hash_max_nnz;
+  return CAS_OK;
+}
+
+cas_status cas_get_tuning(const cas_ctx* ctx, cas_tuning* t) {
+  if (!ctx || !t) return CAS_ERR_BAD_INPUT;
+  t->acc_thres = ctx->acc_thres;
+  t->fusion = ctx->fuse ? 1 : 0;
+  t->fused_min_products = ctx->fused_lo;
+  t->esc_max_products = ctx->esc_max;
+  t->hash_max_nnz = ctx->hash_max;
+  return CAS_OK;
+}
 
 cas_status cas_set_fusion(cas_ctx* ctx, int on) {
   if (!ctx) return CAS_ERR_BAD_INPUT;

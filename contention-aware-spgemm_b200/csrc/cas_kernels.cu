@@ -97,7 +97,7 @@ __device__ __forceinline__ int heavy_class(int64_t flp) {  // 0 for the heaviest
 }
 
 __global__ void k_bin_count_numc(int64_t m, const int64_t* __restrict__ row_flp, const int64_t* __restrict__ crp,
-                                 const int64_t* __restrict__ arp, int mode, double thres,
+                                 const int64_t* __restrict__ arp, int mode, double thres, int esc_max, int hash_max,
                                  unsigned long long* __restrict__ bin_count, unsigned long long* __restrict__ bin_sums,
                                  unsigned long long* __restrict__ heavy_count) {
   __shared__ unsigned long long s_cnt[4 * kNumcBins];
@@ -107,7 +107,7 @@ __global__ void k_bin_count_numc(int64_t m, const int64_t* __restrict__ row_flp,
   __syncthreads();
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
     const int64_t flp = row_flp[r], nz = crp[r + 1] - crp[r];
-    const int b = numc_bin_of(flp, nz, mode, thres);
+    const int b = numc_bin_of(flp, nz, mode, thres, esc_max, hash_max);
     if (b == kNB_Dense) atomicAdd(&s_heavy[heavy_class(flp)], 1ull);
     atomicAdd(&s_cnt[b], 1ull);
     atomicAdd(&s_cnt[kNumcBins + b], (unsigned long long)flp);
@@ -122,11 +122,12 @@ __global__ void k_bin_count_numc(int64_t m, const int64_t* __restrict__ row_flp,
 }
 
 __global__ void k_bin_scatter_numc(int64_t m, const int64_t* __restrict__ row_flp, const int64_t* __restrict__ crp,
-                                   int mode, double thres, unsigned long long* __restrict__ cursor,
+                                   int mode, double thres, int esc_max, int hash_max,
+                                   unsigned long long* __restrict__ cursor,
                                    unsigned long long* __restrict__ heavy_cursor, int32_t* __restrict__ rows) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += (int64_t)gridDim.x * blockDim.x) {
     const int64_t flp = row_flp[r];
-    const int b = numc_bin_of(flp, crp[r + 1] - crp[r], mode, thres);
+    const int b = numc_bin_of(flp, crp[r + 1] - crp[r], mode, thres, esc_max, hash_max);
     const unsigned long long pos =
         b == kNB_Dense ? warp_aggregated_add(heavy_cursor, heavy_class(flp)) : warp_aggregated_add(cursor, b);
     rows[pos] = (int32_t)r;

@@ -70,12 +70,13 @@ struct Csr {
   const void* __restrict__ val;
 };
 
-// Rows with kFusedLo < products <= kFusedHi run through the fused ESC kernel
-// when fusion is on: no symbolic pass, so they sit in the symbolic zero bin.
+// Rows with fuse_lo < products <= kFusedHi run through the fused ESC kernel
+// when fusion is on (fuse_lo > 0; the default lower bound is kFusedLo): no
+// symbolic pass, so they sit in the symbolic zero bin.
 constexpr int64_t kFusedLo = 2048;
 constexpr int64_t kFusedHi = 4800;
-__host__ __device__ __forceinline__ bool fused_row(int64_t flp, int fuse) {
-  return fuse && flp > kFusedLo && flp <= kFusedHi;
+__host__ __device__ __forceinline__ bool fused_row(int64_t flp, int fuse_lo) {
+  return fuse_lo > 0 && flp > fuse_lo && flp <= kFusedHi;
 }
 __host__ __device__ __forceinline__ int symb_bin_of(int64_t flp, int64_t ncol, int fuse = 0) {
   if (flp <= 0 || fused_row(flp, fuse)) return kSB_Zero;
@@ -93,11 +94,15 @@ __host__ __device__ __forceinline__ int symb_bin_of(int64_t flp, int64_t ncol, i
 // Accumulator choice of one row: the hybrid mode takes ESC when the row's
 // compression factor flp/nnz is below the threshold, as
 // ams_hybacc_numc_krnl does (src/ams/ams_utils.c:1139-1149).
-__host__ __device__ __forceinline__ int numc_bin_of(int64_t flp, int64_t nz, int mode, double thres) {
+// esc_max and hash_max (the tuning's limits, at most 8192 and 4096) cap the
+// rows the ESC and hash kernels take; larger rows fall through to the next
+// form.
+__host__ __device__ __forceinline__ int numc_bin_of(int64_t flp, int64_t nz, int mode, double thres,
+                                                    int esc_max = 8192, int hash_max = 4096) {
   if (flp <= 0 || nz <= 0) return kNB_Zero;
   if (flp <= 32) return kNB_Tiny;
   bool esc = mode == kAccEsc || (mode == kAccHybrid && (double)flp / (double)nz < thres);
-  if (esc) {
+  if (esc && flp <= esc_max) {
     if (flp <= 1024) return kNB_E1K;
     if (flp <= 2048) return kNB_E2K;
     if (flp <= 3072) return kNB_E3K;
@@ -106,9 +111,11 @@ __host__ __device__ __forceinline__ int numc_bin_of(int64_t flp, int64_t nz, int
     if (flp <= 6144) return kNB_E6K;
     if (flp <= 8192) return kNB_E8K;
   }
-  if (nz <= 256) return kNB_H256;
-  if (nz <= 1024) return kNB_H1K;
-  if (nz <= 4096) return kNB_H4K;
+  if (nz <= hash_max) {
+    if (nz <= 256) return kNB_H256;
+    if (nz <= 1024) return kNB_H1K;
+    if (nz <= 4096) return kNB_H4K;
+  }
   return kNB_Dense;
 }
 

@@ -120,12 +120,30 @@ cas_status cas_set_stream(cas_ctx *ctx, void *stream);
 cas_status cas_set_acc_thres(cas_ctx *ctx, double thres);
 const char *cas_last_error(const cas_ctx *ctx);
 /* 1 (default): in cas_spgemm with the ESC or hybrid accumulator, rows of
- * 2049..4800 products skip the symbolic pass: one kernel counts, sorts and
+ * 2049..4800 products (the lower bound is cas_tuning.fused_min_products)
+ * skip the symbolic pass: one kernel counts, sorts and
  * places each of them, finding its offset in C from the rows before it, and
  * C is allocated by the bound min(products, columns) for those rows
  * (C->num_nnz is exact; the arrays may be longer).  0: every row has a
  * symbolic pass, as in the reference's drivers.  The output is the same. */
 cas_status cas_set_fusion(cas_ctx *ctx, int on);
+
+/* Routing of rows to kernels, all of it in one place (the defaults in
+ * brackets).  The output never depends on it, only the speed: the
+ * project's autotuner (casgemm.Autotuner) times candidate settings per
+ * degree-distribution class of the inputs and keeps the fastest.
+ * No counterpart in the reference beyond AMS_ACC_THRES, whose
+ * thresholds are compile-time macros (CMakeLists.txt:57-65). */
+typedef struct {
+	double acc_thres;            /* AMS_ACC_THRES of the hybrid accumulator [2.0] */
+	int32_t fusion;              /* fused ESC rows, as cas_set_fusion [1] */
+	int32_t fused_min_products;  /* fused rows have more products than this, up to 4800 [2048] */
+	int32_t esc_max_products;    /* ESC rows have at most this many products, <= 8192 [8192] */
+	int32_t hash_max_nnz;        /* hash rows have at most this many distinct columns, <= 4096 [4096];
+	                                larger rows take the dense kernels */
+} cas_tuning;
+cas_status cas_set_tuning(cas_ctx *ctx, const cas_tuning *t);
+cas_status cas_get_tuning(const cas_ctx *ctx, cas_tuning *t);
 /* 1: run the bins one after another on the context's stream and time every
  * bin kernel with CUDA events (cas_stats.*_bin_ms); 0 (default): bins run
  * concurrently on auxiliary streams. */

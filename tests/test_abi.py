@@ -56,3 +56,11 @@ def test_oracle_library_exports():
     for n in ("orc_flp_populate", "orc_scan", "orc_hash_symb", "orc_spgemm", "orc_radix_sort_kv",
               "orc_pack_morsels", "orc_sort_rows", "orc_intprod"):
         assert hasattr(lib, n)
+
+
+def test_autotuner_key_is_a_function_of_the_degrees():
+    A = casgemm.gen_er(10, 32, 1)
+    G = casgemm.gen_g500(12, 8, 1)
+    assert casgemm.Autotuner.key(A, A) == casgemm.Autotuner.key(casgemm.gen_er(10, 32, 9), casgemm.gen_er(10, 32, 9))
+    assert casgemm.Autotuner.key(A, A) != casgemm.Autotuner.key(G, G)
+    assert casgemm.Autotuner.key(A, A).endswith("_f64")

@@ -144,3 +144,51 @@ def test_profiling_leaves_no_cuda_error(ctx):
         ctx.set_profiling(False)
     assert out.stats["fused_rows"] > 0 and out.stats["fused_ms"] > 0
     torch.zeros(4, device="cuda").sum().item()  # raises if an error is pending
+
+
+def test_tuning_routes_rows_but_not_results(ctx):
+    """cas_set_tuning moves rows between kernels; C stays bit-identical."""
+    A = casgemm.gen_g500(12, 16, 4)
+    B = A.transpose()
+    ref = oracle.oracle_spgemm(A, B, "hybacc")
+    saved = ctx.get_tuning()
+    seen = set()
+    try:
+        for kw in ({"esc_max_products": 1024}, {"hash_max_nnz": 256}, {"fused_min_products": 512},
+                   {"acc_thres": 5.0}, {"fusion": 0}):
+            ctx.set_tuning(**saved)
+            ctx.set_tuning(**kw)
+            out = ctx.spgemm(A, B, "hybacc")
+            same(out, ref)
+            seen.add(tuple(sorted((k, v) for k, v in out.stats["numc_bins"].items() if v)))
+        with pytest.raises(casgemm.CasError):
+            ctx.set_tuning(esc_max_products=9000)
+    finally:
+        ctx.set_tuning(**saved)
+    assert len(seen) >= 3, "the knobs change the routing"
+
+
+def test_autotuner_caches_per_class(ctx, tmp_path):
+    import torch
+    dev = torch.device("cuda", 0)
+
+    def to_dev(M):
+        t = [torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in (M.row_ptrs, M.cols, M.vals)]
+        return casgemm.DeviceCsr(M.num_row, M.num_col, M.nnz, t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(),
+                                 M.val_type, keep=t)
+
+    A = casgemm.gen_er(11, 32, 2)
+    key = casgemm.Autotuner.key(A, A)
+    path = str(tmp_path / "tune.json")
+    tuner = casgemm.Autotuner(ctx, path)
+    before = ctx.get_tuning()
+    cfg = tuner.tune(key, to_dev(A), to_dev(A), trials=1)
+    assert ctx.get_tuning() == before  # tuning leaves the context as it was
+    assert cfg["seconds"] > 0 and cfg["seconds"] <= cfg["default_seconds"]
+    again = casgemm.Autotuner(ctx, path)
+    assert again.apply(key)
+    try:
+        out = ctx.spgemm(A, A.transpose(), "hybacc")
+        same(out, oracle.oracle_spgemm(A, A.transpose(), "hybacc"))
+    finally:
+        ctx.set_tuning(**before)
