@@ -169,6 +169,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "cas_intprod_host": (I64, [I64, P, P, P]),
         "cas_mtx_read": (I64, [ctypes.c_char_p, ctypes.POINTER(I64), ctypes.POINTER(I64), P, P, P]),
         "cas_mtx_write": (I32, [ctypes.c_char_p, I64, I64, P, P, ctypes.c_int]),
+        "cas_csr_write_bin": (I32, [ctypes.c_char_p, I64, I64, P, P, P]),
+        "cas_csr_read_bin": (I64, [ctypes.c_char_p, ctypes.POINTER(I64), ctypes.POINTER(I64), P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -626,6 +628,28 @@ def mtx_write(path: str, A: Csr, symmetric: bool):
     if load().cas_mtx_write(path.encode(), A.num_row, A.num_col, _ptr(np.ascontiguousarray(A.row_ptrs, np.int64)),
                             _ptr(np.ascontiguousarray(A.cols, np.int32)), int(symmetric)) != 0:
         raise ValueError(f"cannot write {path}")
+
+
+def csr_write_bin(path: str, A: Csr):
+    """Binary CSR cache of A (cas_csr_write_bin); fp64 values."""
+    vals = np.ascontiguousarray(A.vals, dtype=np.float64)
+    if load().cas_csr_write_bin(path.encode(), A.num_row, A.num_col, _ptr(np.ascontiguousarray(A.row_ptrs, np.int64)),
+                                _ptr(np.ascontiguousarray(A.cols, np.int32)), _ptr(vals)) != 0:
+        raise ValueError(f"cannot write {path}")
+
+
+def csr_read_bin(path: str) -> Csr:
+    lib = load()
+    nr, nc = ctypes.c_int64(), ctypes.c_int64()
+    nnz = lib.cas_csr_read_bin(path.encode(), ctypes.byref(nr), ctypes.byref(nc), None, None, None)
+    if nnz < 0:
+        raise ValueError(f"cannot read {path}")
+    rp = np.empty(nr.value + 1, np.int64)
+    cols = np.empty(nnz, np.int32)
+    vals = np.empty(nnz, np.float64)
+    if lib.cas_csr_read_bin(path.encode(), ctypes.byref(nr), ctypes.byref(nc), _ptr(rp), _ptr(cols), _ptr(vals)) != nnz:
+        raise ValueError(f"cannot read {path}")
+    return Csr(nr.value, nc.value, rp, cols, vals)
 
 
 # ---------------------------------------------------------- row sharding

@@ -690,3 +690,62 @@ int cas_mtx_write(const char *path, int64_t num_row, int64_t num_col, const int6
 	free(b);
 	return fclose(f) == 0 ? 0 : -1;
 }
+
+/* ------------------------------------------------------- binary CSR cache */
+
+static const char cas_csr_magic[8] = {'C', 'A', 'S', 'C', 'S', 'R', '1', '\0'};
+
+int cas_csr_write_bin(const char *path, int64_t num_row, int64_t num_col, const int64_t *row_ptrs,
+	const int32_t *cols, const double *vals) {
+	if (!path || num_row < 0 || num_col < 0 || !row_ptrs) {
+		return -1;
+	}
+	const int64_t nnz = row_ptrs[num_row] - row_ptrs[0];
+	if (row_ptrs[0] != 0 || nnz < 0 || (nnz > 0 && (!cols || !vals))) {
+		return -1;
+	}
+	FILE *f = fopen(path, "wb");
+	if (!f) {
+		return -1;
+	}
+	const int64_t head[3] = {num_row, num_col, nnz};
+	int ok = fwrite(cas_csr_magic, 1, 8, f) == 8 && fwrite(head, sizeof(int64_t), 3, f) == 3 &&
+		fwrite(row_ptrs, sizeof(int64_t), (size_t) (num_row + 1), f) == (size_t) (num_row + 1) &&
+		(nnz == 0 || (fwrite(cols, sizeof(int32_t), (size_t) nnz, f) == (size_t) nnz &&
+			fwrite(vals, sizeof(double), (size_t) nnz, f) == (size_t) nnz));
+	ok = (fclose(f) == 0) && ok;
+	return ok ? 0 : -1;
+}
+
+int64_t cas_csr_read_bin(const char *path, int64_t *num_row, int64_t *num_col, int64_t *row_ptrs,
+	int32_t *cols, double *vals) {
+	if (!path || !num_row || !num_col) {
+		return -1;
+	}
+	FILE *f = fopen(path, "rb");
+	if (!f) {
+		return -1;
+	}
+	char magic[8];
+	int64_t head[3];
+	if (fread(magic, 1, 8, f) != 8 || memcmp(magic, cas_csr_magic, 8) != 0 ||
+		fread(head, sizeof(int64_t), 3, f) != 3 || head[0] < 0 || head[1] < 0 || head[2] < 0) {
+		fclose(f);
+		return -1;
+	}
+	*num_row = head[0];
+	*num_col = head[1];
+	const int64_t nnz = head[2];
+	if (cols) {
+		if (!row_ptrs || (nnz > 0 && !vals) ||
+			fread(row_ptrs, sizeof(int64_t), (size_t) (head[0] + 1), f) != (size_t) (head[0] + 1) ||
+			(nnz > 0 && (fread(cols, sizeof(int32_t), (size_t) nnz, f) != (size_t) nnz ||
+				fread(vals, sizeof(double), (size_t) nnz, f) != (size_t) nnz)) ||
+			row_ptrs[0] != 0 || row_ptrs[head[0]] != nnz) {
+			fclose(f);
+			return -1;
+		}
+	}
+	fclose(f);
+	return nnz;
+}

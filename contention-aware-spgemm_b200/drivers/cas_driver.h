@@ -30,7 +30,8 @@
  * freed after each run (free_csr).  thread_num reports the GPU's SM count
  * and numa_mask the bit of the CUDA device used.
  *
- * Environment: CAS_DATASET_DIR (default ./dataset), CAS_RUN_NUM (default 10,
+ * Environment: CAS_DATASET_DIR (default ./dataset), CAS_CSR_CACHE (1: keep
+ * and reuse a binary <dataset>.org.csr / .trs.csr beside the .mtx files), CAS_RUN_NUM (default 10,
  * at least 2, the reference's RUN_NUM), CAS_DEVICE (default 0),
  * CAS_VERIFY (1: VERIFYRESULT lines), CAS_ACC_THRES (hybrid threshold,
  * default 2.0 = the R-MAT scripts' value), CAS_PEAK_GBS (HBM bandwidth for
@@ -72,9 +73,40 @@ static double drv_env_double(const char *name, double dflt) {
 	return (s && *s) ? strtod(s, NULL) : dflt;
 }
 
-/* Host CSR from a MatrixMarket file (two-phase cas_mtx_read). */
+/* Host CSR from a MatrixMarket file (two-phase cas_mtx_read), or from its
+ * binary cache <path without .mtx>.csr when CAS_CSR_CACHE is 1 (written on
+ * the first run, read on the later ones). */
 static void drv_load(const char *path, cas_csr *M) {
 	int64_t nr = 0, nc = 0;
+	char bin[CAS_DRIVER_PATH_LEN];
+	const int cache = (int)drv_env_long("CAS_CSR_CACHE", 0);
+	snprintf(bin, sizeof(bin), "%s", path);
+	char *dot = strrchr(bin, '.');
+	if (dot && !strcmp(dot, ".mtx")) strcpy(dot, ".csr");
+	if (cache) {
+		const int64_t bnnz = cas_csr_read_bin(bin, &nr, &nc, NULL, NULL, NULL);
+		if (bnnz >= 0) {
+			int64_t *rp = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nr + 1));
+			int32_t *cols = (int32_t *)malloc(sizeof(int32_t) * (size_t)(bnnz > 0 ? bnnz : 1));
+			double *vals = (double *)malloc(sizeof(double) * (size_t)(bnnz > 0 ? bnnz : 1));
+			if (!rp || !cols || !vals) drv_die("host allocation failed");
+			if (cas_csr_read_bin(bin, &nr, &nc, rp, cols, vals) == bnnz) {
+				memset(M, 0, sizeof(*M));
+				M->num_row = nr;
+				M->num_col = nc;
+				M->num_nnz = bnnz;
+				M->row_ptrs = rp;
+				M->cols = cols;
+				M->rats = vals;
+				M->col_bytes = 4;
+				M->val_type = CAS_VAL_F64;
+				return;
+			}
+			free(rp);
+			free(cols);
+			free(vals);
+		}
+	}
 	const int64_t nnz = cas_mtx_read(path, &nr, &nc, NULL, NULL, NULL);
 	if (nnz < 0) {
 		fprintf(stderr, "Error opening or parsing %s\n", path);
@@ -85,6 +117,8 @@ static void drv_load(const char *path, cas_csr *M) {
 	double *vals = (double *)malloc(sizeof(double) * (size_t)(nnz > 0 ? nnz : 1));
 	if (!rp || !cols || !vals) drv_die("host allocation failed");
 	if (cas_mtx_read(path, &nr, &nc, rp, cols, vals) != nnz) drv_die("MatrixMarket reread failed");
+	if (cache && cas_csr_write_bin(bin, nr, nc, rp, cols, vals) != 0)
+		fprintf(stderr, "warning: could not write the CSR cache %s\n", bin);
 	memset(M, 0, sizeof(*M));
 	M->num_row = nr;
 	M->num_col = nc;

@@ -75,6 +75,18 @@ int64_t cas_mtx_read(const char *path, int64_t *num_row, int64_t *num_col,
 int cas_mtx_write(const char *path, int64_t num_row, int64_t num_col, const int64_t *row_ptrs,
 	const int32_t *cols, int symmetric);
 
+/* Binary CSR cache, so a dataset is parsed from MatrixMarket once: the
+ * bytes "CASCSR1" and a NUL, then num_row, num_col and nnz as int64, then
+ * row_ptrs (num_row + 1 int64), cols (nnz int32) and vals (nnz double), all
+ * little-endian.  No counterpart in the reference, which parses the .mtx
+ * files on every run (raw2csr, src/mm/mm_utils.c:451-692).  Write returns 0
+ * or -1.  Read is two-phase like cas_mtx_read (cols == NULL returns nnz and
+ * the shape) and returns nnz, or -1 on a missing or malformed file. */
+int cas_csr_write_bin(const char *path, int64_t num_row, int64_t num_col, const int64_t *row_ptrs,
+	const int32_t *cols, const double *vals);
+int64_t cas_csr_read_bin(const char *path, int64_t *num_row, int64_t *num_col, int64_t *row_ptrs,
+	int32_t *cols, double *vals);
+
 #ifdef __cplusplus
 }
 #endif

@@ -103,3 +103,17 @@ def test_mtx_roundtrip(tmp_path):
     casgemm.mtx_write(q, Z.transpose(), symmetric=False)
     T = casgemm.mtx_read(q)
     assert (T.to_scipy() != Z.to_scipy().T).nnz == 0
+
+
+def test_binary_csr_cache_roundtrip(tmp_path):
+    Z = casgemm.gen_zipf(400, 900, 80, 3000, 6, col_q=5.0)
+    p = str(tmp_path / "z.csr")
+    casgemm.csr_write_bin(p, Z)
+    R = casgemm.csr_read_bin(p)
+    assert (R.num_row, R.num_col) == (Z.num_row, Z.num_col)
+    np.testing.assert_array_equal(R.row_ptrs, Z.row_ptrs)
+    np.testing.assert_array_equal(R.cols, Z.cols)
+    np.testing.assert_array_equal(R.vals, Z.vals)
+    open(p, "r+b").write(b"XX")  # a damaged header is refused, not misread
+    with pytest.raises(ValueError):
+        casgemm.csr_read_bin(p)

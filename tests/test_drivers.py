@@ -97,7 +97,7 @@ def test_driver_matches_reference_log(tmp_path, algo):
     ds = tmp_path / "dataset"
     subprocess.run([os.path.join(BIN, "cas_gen"), "g500", "12", "8"], check=True, capture_output=True,
                    env=dict(os.environ, CAS_DATASET_DIR=str(ds)))
-    env = dict(os.environ, CAS_RUN_NUM="3", CAS_VERIFY="1")
+    env = dict(os.environ, CAS_RUN_NUM="3", CAS_VERIFY="1", CAS_CSR_CACHE="1")
     p = subprocess.run([os.path.join(BIN, ALGOS[algo]), "g500_12_8"], cwd=tmp_path, capture_output=True, text=True,
                        env=env, timeout=300)
     assert p.returncode == 0, p.stderr
@@ -116,3 +116,9 @@ def test_driver_matches_reference_log(tmp_path, algo):
     assert dict(ours)["flop_cnt"] == dict(theirs)["flop_cnt"]
     assert dict(ours)["dataset"] == "g500_12_8" and dict(ours)["num_trials"] == "2"
     assert [k for k, _ in ours[len(theirs):]] == ["gflops", "hbm_frac", "device"]
+    # the binary cache written by this run serves the next one with the same result
+    assert (ds / "g500_12_8.org.csr").exists() and (ds / "g500_12_8.trs.csr").exists()
+    q = subprocess.run([os.path.join(BIN, ALGOS[algo]), "g500_12_8"], cwd=tmp_path, capture_output=True, text=True,
+                       env=env, timeout=300)
+    assert q.returncode == 0, q.stderr
+    assert set(verify_triples(q.stdout)) == set(verify_triples(ref))
