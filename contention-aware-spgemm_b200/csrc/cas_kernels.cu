@@ -881,6 +881,15 @@ __device__ __forceinline__ int sort_compact_small(uint32_t* __restrict__ skey, A
   return h;
 }
 
+// Sorts the pairs of one bucket [s, e), e - s <= 128, by key with the whole
+// warp and leaves the distinct (key, sum) pairs at [s, s + heads), kEmptyKey
+// behind them; returns heads.  A rank sort (a pair's rank counts the smaller
+// keys and the equal keys before it, so equal keys keep their order) puts the
+// pairs in order; a segmented inclusive scan over each 32-pair row of the
+// sorted order (Hillis-Steele, segments start at the first pair of each key),
+// carried from row to row, gives every run's sum at its last pair.  No two
+// lanes add into the same slot, so a run of one key (the diagonal column of
+// A*A^T brings one per A entry) costs no more than distinct keys.
 template <typename AT>
 __device__ __forceinline__ int warp_sort_compact(uint32_t* __restrict__ skey, AT* __restrict__ sval, int s, int e) {
   constexpr int PER = 4;
@@ -896,6 +905,7 @@ __device__ __forceinline__ int warp_sort_compact(uint32_t* __restrict__ skey, AT
     v[i] = idx < b ? sval[s + idx] : AT(0);
     rk[i] = 0;
   }
+#pragma unroll 4
   for (int j = 0; j < b; ++j) {
     const uint32_t kj = skey[s + j];
 #pragma unroll
@@ -912,30 +922,42 @@ __device__ __forceinline__ int warp_sort_compact(uint32_t* __restrict__ skey, AT
   __syncwarp();
   int heads = 0;
   int run[PER];
-  bool hd[PER];
+  bool hd[PER], last[PER];
+  AT carry = AT(0);
 #pragma unroll
   for (int i = 0; i < PER; ++i) {
     const int t = lane + 32 * i;
-    k[i] = t < b ? skey[s + t] : kEmptyKey;
-    v[i] = t < b ? sval[s + t] : AT(0);
-    const uint32_t kp = (t > 0 && t < b) ? skey[s + t - 1] : ~k[i];
-    hd[i] = t < b && k[i] != kp;
+    const bool in = t < b;
+    k[i] = in ? skey[s + t] : kEmptyKey;
+    AT x = in ? sval[s + t] : AT(0);
+    const uint32_t kp = (t > 0 && in) ? skey[s + t - 1] : ~k[i];
+    const uint32_t kn = (t + 1 < b) ? skey[s + t + 1] : ~k[i];
+    hd[i] = in && k[i] != kp;
+    last[i] = in && k[i] != kn;
     const unsigned m = __ballot_sync(kFull, hd[i]);
     run[i] = heads + __popc(m & ((lanemask_lt() << 1) | 1u)) - 1;
     heads += __popc(m);
+    // segmented scan of the row; pairs past the bucket start segments of their own
+    bool f = hd[i] || !in;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const AT y = __shfl_up_sync(kFull, x, d);
+      const bool g = __shfl_up_sync(kFull, (int)f, d) != 0;
+      if (lane >= d) {
+        if (!f) x = y + x;
+        f = f || g;
+      }
+    }
+    if (!f) x = carry + x;  // the run continues from the previous row
+    carry = __shfl_sync(kFull, x, 31);
+    v[i] = x;
   }
   __syncwarp();
 #pragma unroll
   for (int i = 0; i < PER; ++i) {
-    if (hd[i]) {
-      skey[s + run[i]] = k[i];
-      sval[s + run[i]] = AT(0);
-    }
+    if (hd[i]) skey[s + run[i]] = k[i];
+    if (last[i]) sval[s + run[i]] = v[i];
   }
-  __syncwarp();
-#pragma unroll
-  for (int i = 0; i < PER; ++i)
-    if (lane + 32 * i < b) atomic_add_sh(&sval[s + run[i]], v[i]);
   for (int t = heads + lane; t < b; t += 32) skey[s + t] = kEmptyKey;
   __syncwarp();
   return heads;
@@ -959,7 +981,6 @@ __device__ __forceinline__ int warp_sort_compact(uint32_t* __restrict__ skey, AT
 // column of A*A^T alone puts |A_i| products into one bucket.  Shared memory:
 // 13 bytes per product plus half a byte per bucket.
 constexpr int kBucketLimit = 128;
-constexpr int kBigBuckets = 256;  // buckets of more than 8 pairs one row may have
 // Buckets of more than kBucketLimit pairs that span at most kHugeWidth
 // columns (hub columns of a skewed graph, repeated many times) are summed
 // by the whole block into a dense kHugeWidth-slot array over the byte
@@ -1214,11 +1235,13 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   }
   __syncthreads();
   // sort each bucket, sum equal columns, compact them to the bucket front:
-  // one lane per bucket of at most 8 pairs; larger buckets (about 1 in 100,
-  // and the diagonal column's) are queued for a whole warp each
-  __shared__ uint16_t s_big[kBigBuckets], s_huge[kHugeBuckets];
-  __shared__ int s_nbig, s_nhuge;
-  if (threadIdx.x == 0) s_nbig = s_nhuge = 0;
+  // one lane per bucket of at most 8 pairs; the warp then takes its larger
+  // buckets (about 1 in 100, and the diagonal column's) one at a time, so
+  // they overlap the other warps' small buckets.  Buckets of more than
+  // kBucketLimit pairs are queued for the whole block.
+  __shared__ uint16_t s_huge[kHugeBuckets];
+  __shared__ int s_nhuge;
+  if (threadIdx.x == 0) s_nhuge = 0;
   __syncthreads();
   for (int g = warp; g < NG; g += NW) {
     const int b = g * 32 + lane;
@@ -1226,9 +1249,6 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
     if (e - s > kBucketLimit) {
       const int slot = atomicAdd(&s_nhuge, 1);
       if (slot < kHugeBuckets) s_huge[slot] = (uint16_t)b;
-    } else if (e - s > 8) {
-      const int slot = atomicAdd(&s_nbig, 1);
-      if (slot < kBigBuckets) s_big[slot] = (uint16_t)b;
     }
     // one network size for the whole warp: the smallest that fits its
     // largest bucket of at most 8 pairs
@@ -1239,17 +1259,16 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
       else if (mx <= 6) sort_compact_small<6, AT>(skey, sval, s, e);
       else sort_compact_small<8, AT>(skey, sval, s, e);
     }
+    for (unsigned big = __ballot_sync(kFull, e - s > 8 && e - s <= kBucketLimit); big; big &= big - 1) {
+      const int l = __ffs(big) - 1;
+      warp_sort_compact<AT>(skey, sval, __shfl_sync(kFull, s, l), __shfl_sync(kFull, e, l));
+    }
   }
   __syncthreads();
-  if (s_nbig > kBigBuckets || s_nhuge > kHugeBuckets) {  // uniform: too many large buckets for this form
+  if (s_nhuge > kHugeBuckets) {  // uniform: too many huge buckets for this form
     if (FUSED) count_and_defer();
     else if (threadIdx.x == 0) ovf[atomicAdd(ovf_count, 1u)] = (int32_t)r;
     return;
-  }
-  for (int i = warp; i < s_nbig; i += NW) {
-    const int b = s_big[i];
-    const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
-    warp_sort_compact<AT>(skey, sval, s, e);
   }
   if (s_nhuge > 0) {
     // the whole block, one huge bucket at a time: sums by column offset in a
