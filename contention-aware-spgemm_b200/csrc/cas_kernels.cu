@@ -1,5 +1,6 @@
 // casgemm kernel bodies (contracts in cas_kernels.cuh).
 #include "cas_kernels.cuh"
+#include "cas_sortnet.cuh"
 
 namespace cas {
 
@@ -725,42 +726,6 @@ __device__ __forceinline__ uint32_t bucket_add(uint32_t* w, int b) {
 }
 __device__ __forceinline__ uint32_t bucket_get(const uint32_t* w, int b) { return (w[b >> 1] >> ((b & 1) << 4)) & 0xFFFFu; }
 
-__device__ __forceinline__ void cswap(uint32_t& ka, uint32_t& pa, uint32_t& kb, uint32_t& pb) {
-  const bool sw = kb < ka;
-  const uint32_t k0 = sw ? kb : ka, k1 = sw ? ka : kb, p0 = sw ? pb : pa, p1 = sw ? pa : pb;
-  ka = k0; kb = k1; pa = p0; pb = p1;
-}
-
-// Batcher's odd-even merge sort network for 8 inputs (19 comparators).
-__device__ __forceinline__ void sort8(uint32_t (&k)[8], uint32_t (&p)[8]) {
-  cswap(k[0], p[0], k[1], p[1]); cswap(k[2], p[2], k[3], p[3]);
-  cswap(k[4], p[4], k[5], p[5]); cswap(k[6], p[6], k[7], p[7]);
-  cswap(k[0], p[0], k[2], p[2]); cswap(k[1], p[1], k[3], p[3]);
-  cswap(k[4], p[4], k[6], p[6]); cswap(k[5], p[5], k[7], p[7]);
-  cswap(k[1], p[1], k[2], p[2]); cswap(k[5], p[5], k[6], p[6]);
-  cswap(k[0], p[0], k[4], p[4]); cswap(k[1], p[1], k[5], p[5]);
-  cswap(k[2], p[2], k[6], p[6]); cswap(k[3], p[3], k[7], p[7]);
-  cswap(k[2], p[2], k[4], p[4]); cswap(k[3], p[3], k[5], p[5]);
-  cswap(k[1], p[1], k[2], p[2]); cswap(k[3], p[3], k[4], p[4]);
-  cswap(k[5], p[5], k[6], p[6]);
-}
-// Optimal networks for 4 (5 comparators) and 6 inputs (12 comparators), for
-// warps whose buckets are all small; all three are checked exhaustively on
-// 0/1 inputs by the 0-1 principle.
-__device__ __forceinline__ void sort_net(uint32_t (&k)[4], uint32_t (&p)[4]) {
-  cswap(k[0], p[0], k[1], p[1]); cswap(k[2], p[2], k[3], p[3]);
-  cswap(k[0], p[0], k[2], p[2]); cswap(k[1], p[1], k[3], p[3]);
-  cswap(k[1], p[1], k[2], p[2]);
-}
-__device__ __forceinline__ void sort_net(uint32_t (&k)[6], uint32_t (&p)[6]) {
-  cswap(k[0], p[0], k[5], p[5]); cswap(k[1], p[1], k[3], p[3]); cswap(k[2], p[2], k[4], p[4]);
-  cswap(k[1], p[1], k[2], p[2]); cswap(k[3], p[3], k[4], p[4]);
-  cswap(k[0], p[0], k[3], p[3]); cswap(k[2], p[2], k[5], p[5]);
-  cswap(k[0], p[0], k[1], p[1]); cswap(k[2], p[2], k[3], p[3]); cswap(k[4], p[4], k[5], p[5]);
-  cswap(k[1], p[1], k[2], p[2]); cswap(k[3], p[3], k[4], p[4]);
-}
-__device__ __forceinline__ void sort_net(uint32_t (&k)[8], uint32_t (&p)[8]) { sort8(k, p); }
-
 // Products of a staged chunk too large for the byte table: the A entry of
 // product p is found by binary search over the 32-bit prefixes.
 template <int BLOCK, typename VIn, typename F>
@@ -840,41 +805,41 @@ __device__ __forceinline__ void atomic_add_sh(long long* p, long long v) {
 }
 
 // Sorts the (key, value) pairs of one bucket [s, e), 1 <= e - s <= N, in
-// shared memory by key with the N-input network in registers, sums equal
-// keys, and leaves the distinct (key, sum) pairs at [s, s + heads) and
-// kEmptyKey behind them; returns heads.  One lane per bucket; the caller
-// picks N from the largest bucket of the warp.
+// shared memory by key with the N-input network of cas_sortnet.cuh on packed
+// (key - kbase, slot) words, sums equal keys, and leaves the distinct (key,
+// sum) pairs at [s, s + heads) and kEmptyKey behind them; returns heads.  All
+// keys of the bucket lie in [kbase, kbase + 2^23).  One lane per bucket; the
+// caller picks N from the largest bucket of the warp.
 template <int N, typename AT>
-__device__ __forceinline__ int sort_compact_small(uint32_t* __restrict__ skey, AT* __restrict__ sval, int s, int e) {
+__device__ __forceinline__ int sort_compact_small(uint32_t* __restrict__ skey, AT* __restrict__ sval, int s, int e,
+                                                  uint32_t kbase) {
   const int nb = e - s;
-  uint32_t k[N], q[N];
+  uint32_t w[N];
 #pragma unroll
-  for (int i = 0; i < N; ++i) {
-    k[i] = i < nb ? skey[s + i] : 0xFFFFFFFFu;
-    q[i] = (uint32_t)i;
-  }
-  sort_net(k, q);
+  for (int i = 0; i < N; ++i) w[i] = i < nb ? sortnet_pack(skey[s + i] - kbase, i) : 0xFFFFFFFFu;
+  sort_net(w);
   AT v[N];
 #pragma unroll
-  for (int i = 0; i < N; ++i) v[i] = i < nb ? sval[s + q[i]] : AT(0);
+  for (int i = 0; i < N; ++i) v[i] = i < nb ? sval[s + sortnet_slot(w[i])] : AT(0);
   int h = 0;
-  uint32_t prev = k[0];
+  uint32_t prev = sortnet_offset(w[0]);
   AT acc = v[0];
 #pragma unroll
   for (int i = 1; i < N; ++i) {
     if (i < nb) {
-      if (k[i] != prev) {
-        skey[s + h] = prev;
+      const uint32_t k = sortnet_offset(w[i]);
+      if (k != prev) {
+        skey[s + h] = kbase + prev;
         sval[s + h] = acc;
         ++h;
-        prev = k[i];
+        prev = k;
         acc = v[i];
       } else {
         acc += v[i];
       }
     }
   }
-  skey[s + h] = prev;
+  skey[s + h] = kbase + prev;
   sval[s + h] = acc;
   ++h;
   for (int i = h; i < nb; ++i) skey[s + i] = kEmptyKey;
@@ -1255,9 +1220,10 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
     const int small = (e - s <= 8) ? e - s : 0;
     const int mx = __reduce_max_sync(kFull, small);
     if (small > 0) {
-      if (mx <= 4) sort_compact_small<4, AT>(skey, sval, s, e);
-      else if (mx <= 6) sort_compact_small<6, AT>(skey, sval, s, e);
-      else sort_compact_small<8, AT>(skey, sval, s, e);
+      const uint32_t kbase = lo + ((uint32_t)b << shift);
+      if (mx <= 4) sort_compact_small<4, AT>(skey, sval, s, e, kbase);
+      else if (mx <= 6) sort_compact_small<6, AT>(skey, sval, s, e, kbase);
+      else sort_compact_small<8, AT>(skey, sval, s, e, kbase);
     }
     for (unsigned big = __ballot_sync(kFull, e - s > 8 && e - s <= kBucketLimit); big; big &= big - 1) {
       const int l = __ffs(big) - 1;
