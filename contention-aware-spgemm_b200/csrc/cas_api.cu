@@ -67,6 +67,7 @@ struct cas_ctx {
   bool profile = false;
   bool fuse = true;                        // fused ESC rows (no symbolic pass) in cas_spgemm
   int fused_lo = (int)cas::kFusedLo;       // fused rows: more products than this (up to kFusedHi)
+  int fused_form = 1;                      // fused kernel: 1 index form (k_numc_esc_idx), 0 k_numc_esc_msd
   int esc_max = 8192;                      // ESC rows: at most this many products
   int hash_max = 4096;                     // hash rows: at most this many distinct columns
   double acc_thres = 2.0;
@@ -180,6 +181,13 @@ constexpr size_t smem_numc_esc_msd() {
          ((size_t(CAP) + 15) & ~size_t(15)) + sizeof(cas::StageB<VIn>);
 }
 
+// index form: column, product index and place per product, padded chunk counts
+template <int CAP, int NBB, typename VIn>
+constexpr size_t smem_numc_esc_idx() {
+  return size_t(CAP) * 8 + (size_t(1) << NBB) * 2 + size_t((CAP / 32 + 3) & ~3) * 4 +
+         ((size_t(CAP) + 15) & ~size_t(15)) + sizeof(cas::StageB<VIn>);
+}
+
 // symbolic hash shape of each symbolic bin: threads, log2(table slots), byte
 // table capacity (shared memory allows 3 CTAs per SM for the 16 Ki table)
 #define CAS_SYMB_SHAPES(X)        \
@@ -211,6 +219,8 @@ cas_status setup_numc_kernels(cas_ctx* ctx) {
 #undef CAS_SETUP_ESC
   CAS_TRY(allow_smem(ctx, k_numc_esc_msd<256, (int)kFusedHi, 11, VIn, true>,
                      smem_numc_esc_msd<(int)kFusedHi, 11, VIn>()));
+  CAS_TRY(allow_smem(ctx, k_numc_esc_idx<256, (int)kFusedHi, 11, VIn, true>,
+                     smem_numc_esc_idx<(int)kFusedHi, 11, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_esc_overflow<1024, 8192, VIn>, smem_numc_esc<1024, 8192, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_hash<256, 9, VIn>, smem_numc_hash<256, 9, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_hash<256, 11, VIn>, smem_numc_hash<256, 11, VIn>()));
@@ -658,10 +668,16 @@ cas_status launch_fused(cas_ctx* ctx, Call& c, const int64_t* known, int32_t* cc
   CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + kSlotFused + 4, 0, sizeof(unsigned long long), ctx->stream));
   Fused fu{c.frows, ctx->d_counts + kSlotFused + 4, c.fstatus, known, c.row_nz, cap};
   if (ctx->profile) CAS_CUDA(ctx, cudaEventRecord(ctx->ev_fused[0], ctx->stream));
-  k_numc_esc_msd<256, (int)kFusedHi, 11, VIn, true>
-      <<<(unsigned)c.nf, 256, smem_numc_esc_msd<(int)kFusedHi, 11, VIn>(), ctx->stream>>>(
-          nullptr, c.A.csr, c.B.csr, c.b_sorted ? 1 : 0, nullptr, ccol, static_cast<AT*>(cval), c.ovf, ovf_count,
-          ctx->d_status, fu);
+  if (ctx->fused_form == 1)
+    k_numc_esc_idx<256, (int)kFusedHi, 11, VIn, true>
+        <<<(unsigned)c.nf, 256, smem_numc_esc_idx<(int)kFusedHi, 11, VIn>(), ctx->stream>>>(
+            nullptr, c.A.csr, c.B.csr, c.b_sorted ? 1 : 0, nullptr, ccol, static_cast<AT*>(cval), c.ovf, ovf_count,
+            ctx->d_status, fu);
+  else
+    k_numc_esc_msd<256, (int)kFusedHi, 11, VIn, true>
+        <<<(unsigned)c.nf, 256, smem_numc_esc_msd<(int)kFusedHi, 11, VIn>(), ctx->stream>>>(
+            nullptr, c.A.csr, c.B.csr, c.b_sorted ? 1 : 0, nullptr, ccol, static_cast<AT*>(cval), c.ovf, ovf_count,
+            ctx->d_status, fu);
   CAS_TRY(check_launch(ctx, "k_numc_esc_msd (fused)"));
   if (ctx->profile) CAS_CUDA(ctx, cudaEventRecord(ctx->ev_fused[1], ctx->stream));
   return CAS_OK;
@@ -1127,13 +1143,15 @@ const char* cas_last_error(const cas_ctx* ctx) { return ctx ? ctx->err.c_str() :
 cas_status cas_set_tuning(cas_ctx* ctx, const cas_tuning* t) {
   if (!ctx || !t) return CAS_ERR_BAD_INPUT;
   if (!(t->acc_thres >= 0.0) || t->fused_min_products < 32 || t->fused_min_products >= (int)cas::kFusedHi ||
-      t->esc_max_products < 32 || t->esc_max_products > 8192 || t->hash_max_nnz < 0 || t->hash_max_nnz > 4096)
+      t->esc_max_products < 32 || t->esc_max_products > 8192 || t->hash_max_nnz < 0 || t->hash_max_nnz > 4096 ||
+      (t->fused_form != 0 && t->fused_form != 1))
     return set_err(ctx, CAS_ERR_BAD_INPUT, "tuning out of range");
   ctx->acc_thres = t->acc_thres;
   ctx->fuse = t->fusion != 0;
   ctx->fused_lo = t->fused_min_products;
   ctx->esc_max = t->esc_max_products;
   ctx->hash_max = t->hash_max_nnz;
+  ctx->fused_form = t->fused_form;
   return CAS_OK;
 }
 
@@ -1144,6 +1162,7 @@ cas_status cas_get_tuning(const cas_ctx* ctx, cas_tuning* t) {
   t->fused_min_products = ctx->fused_lo;
   t->esc_max_products = ctx->esc_max;
   t->hash_max_nnz = ctx->hash_max;
+  t->fused_form = ctx->fused_form;
   return CAS_OK;
 }
 

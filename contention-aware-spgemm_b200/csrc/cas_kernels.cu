@@ -1325,6 +1325,397 @@ k_numc_esc_msd(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
     dev_report(st, distinct > nz ? kDevRowOverflow : kDevRowUnderflow, 14, r);
 }
 
+// ---- index form of the bucketed ESC kernel ---------------------------------
+// For rows whose A entries fit one staged chunk (at most kBChunk).  Shared
+// memory holds each product's column (4 bytes), its product index (2 bytes)
+// and later its place in the row (2 bytes) instead of its column and value
+// (12 bytes), so more rows are resident per SM; the kernel is bound by load
+// and barrier latency, which more resident rows hide.  The steps are those
+// of k_numc_esc_msd (ams_hsersc_numc_krnl, src/ams/ams_utils.c:399-456): a
+// keys-only histogram into 2^NBB buckets, a second keys-only expansion that
+// scatters (column, product index) into bucket order, and a sort of each
+// bucket: a network per lane for buckets of up to 8, a warp rank sort for up
+// to kBucketLimit, and a dense sum by the whole block for one bucket of more
+// over at most kHugeWidth columns.  Equal columns stay side by side.  A pass
+// in sorted order writes each distinct column to C and records, for every
+// product, the place of its column in the row; a last pass in product order
+// loads the B values (whole sectors, as the B rows lie in memory) and stores
+// each product a_ik * b_kj at its place, with a global atomic add where
+// several products share a column (the place is zeroed first).  A row with
+// more A entries than one chunk, with two or more buckets of more than
+// kBucketLimit products, or with one that spans more than kHugeWidth
+// columns, is counted with a shared-memory hash and left to the radix-sort
+// ESC kernel (appended to `ovf`), as in k_numc_esc_msd.
+constexpr int kIdxMinBlocks = 4;
+
+// Values of the staged chunk's products only (no columns): f(a, b, p).
+template <int BLOCK, typename VIn, typename F>
+__device__ __forceinline__ void expand_values(const Csr& B, int total, const StageB<VIn>& sg,
+                                              const uint8_t* __restrict__ segof, F&& f) {
+  const VIn* __restrict__ bval = static_cast<const VIn*>(B.val);
+  for (int p0 = threadIdx.x; p0 < total; p0 += BLOCK * kUnroll) {
+    VIn bv[kUnroll];
+    int sgi[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int p = p0 + u * BLOCK;
+      sgi[u] = -1;
+      if (p < total) {
+        const int s = segof[p];
+        bv[u] = __ldg(bval + sg.bs[s] + (p - sg.pre[s]));
+        sgi[u] = s;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u)
+      if (sgi[u] >= 0) f(sg.av[sgi[u]], bv[u], p0 + u * BLOCK);
+  }
+}
+
+template <int N>
+__device__ __forceinline__ void sort_perm_small(uint32_t* __restrict__ skey, uint16_t* __restrict__ sidx, int s, int e,
+                                                uint32_t kbase) {
+  const int nb = e - s;
+  uint32_t w[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) w[i] = i < nb ? sortnet_pack(skey[s + i] - kbase, i) : 0xFFFFFFFFu;
+  sort_net(w);
+  uint16_t q[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) q[i] = i < nb ? sidx[s + sortnet_slot(w[i])] : uint16_t(0);
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    if (i < nb) {
+      skey[s + i] = kbase + sortnet_offset(w[i]);
+      sidx[s + i] = q[i];
+    }
+  }
+}
+
+// Whole-warp stable rank sort of one bucket [s, e), e - s <= 128, of
+// (column, product index) pairs.
+__device__ __forceinline__ void warp_sort_perm(uint32_t* __restrict__ skey, uint16_t* __restrict__ sidx, int s, int e) {
+  constexpr int PER = 4;
+  const int lane = threadIdx.x & 31;
+  const int b = e - s;
+  uint32_t k[PER];
+  uint16_t q[PER];
+  int rk[PER];
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    const int t = lane + 32 * i;
+    k[i] = t < b ? skey[s + t] : kEmptyKey;
+    q[i] = t < b ? sidx[s + t] : uint16_t(0);
+    rk[i] = 0;
+  }
+#pragma unroll 4
+  for (int j = 0; j < b; ++j) {
+    const uint32_t kj = skey[s + j];
+#pragma unroll
+    for (int i = 0; i < PER; ++i) rk[i] += (kj < k[i]) || (kj == k[i] && j < lane + 32 * i);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    if (lane + 32 * i < b) {
+      skey[s + rk[i]] = k[i];
+      sidx[s + rk[i]] = q[i];
+    }
+  }
+  __syncwarp();
+}
+
+template <int BLOCK, int CAP, int NBB, typename VIn, bool FUSED = false>
+__global__ void __launch_bounds__(BLOCK, kIdxMinBlocks)
+k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted, const int64_t* __restrict__ crp,
+               int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval,
+               int32_t* __restrict__ ovf, unsigned int* __restrict__ ovf_count, DevStatus* st, Fused fu) {
+  using AT = typename Acc<VIn>::T;
+  constexpr int NB = 1 << NBB;
+  constexpr int NW = BLOCK / 32;
+  constexpr int NG = NB / 32;
+  constexpr int NCH = CAP / 32;
+  constexpr int NCHP = (NCH + 3) & ~3;  // chunk counts padded to 16 bytes
+  constexpr int ACH = BLOCK < kBChunk ? BLOCK : kBChunk;
+  // the hash of deferred rows spans columns, indices, places, bucket and chunk counts
+  constexpr int TS = floor_pow2((CAP * 8 + NB * 2 + NCHP * 4) / 4);
+  constexpr int TB = __builtin_ctz(TS);
+  static_assert(CAP < 32768 && CAP % 32 == 0, "16-bit counters, product indices and places");
+  static_assert(NG <= BLOCK && NCH <= BLOCK && NB % (2 * BLOCK) == 0, "one count per thread in the scans");
+  static_assert(TS >= CAP + CAP / 4, "hash of deferred rows: load at most 0.8");
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint32_t* skey = reinterpret_cast<uint32_t*>(smem);
+  uint16_t* sidx = reinterpret_cast<uint16_t*>(skey + CAP);
+  uint16_t* place_of = sidx + CAP;                             // per product: its column's place in the row
+  uint32_t* bcnt = reinterpret_cast<uint32_t*>(place_of + CAP);  // NB 16-bit counters
+  uint32_t* ccnt = bcnt + NB / 2;                              // NCH head counts / offsets
+  uint8_t* segof = reinterpret_cast<uint8_t*>(ccnt + NCHP);
+  StageB<VIn>& sg = *reinterpret_cast<StageB<VIn>*>(segof + ((CAP + 15) & ~15));
+  __shared__ long long s_tick, s_off;
+  __shared__ int s_huge, s_hlast;
+  __shared__ uint32_t s_hkb;       // first column of the huge bucket
+  __shared__ AT hsum[kHugeWidth];  // the huge bucket's sums by column offset
+  __shared__ uint32_t hmask[kHugeWidth / 32];
+  __shared__ int hpre[kHugeWidth / 32 + 1];
+  constexpr uint16_t kFromSum = 0xFFFE, kNoProduct = 0xFFFF;
+  static_assert(CAP < kFromSum, "product indices below the markers");
+  // place_of: bit 15 set when the column has several products (atomic add);
+  // kSkip for products of the huge bucket, summed in hsum
+  constexpr uint16_t kShared = 0x8000, kSkip = 0xFFFF;
+  // a_ik * b_kj of product p of the staged chunk (0 for a filler slot)
+  auto slot_value = [&](uint16_t p) -> AT {
+    if (p == kNoProduct) return AT(0);
+    const int sgi = segof[p];
+    return Acc<VIn>::mul(sg.av[sgi], __ldg(static_cast<const VIn*>(B.val) + sg.bs[sgi] + ((int)p - sg.pre[sgi])));
+  };
+  int64_t r, tick = 0;
+  if (FUSED) {
+    if (threadIdx.x == 0) s_tick = (long long)atomicAdd(fu.ticket, 1ull);
+    __syncthreads();
+    tick = s_tick;
+    r = fu.rows[tick];
+  } else {
+    r = rows[blockIdx.x];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t as = A.rp[r], ae = A.rp[r + 1];
+  // fused rows: publish `cnt` and return the row's first position in C (-1
+  // when the look-back gave up)
+  auto place = [&](long long cnt) -> long long {
+    if (warp == 0) {
+      const long long ex = lookback_prefix(fu.status, tick, cnt);
+      if (lane == 0) {
+        s_off = ex < 0 ? -1 : (long long)fu.known[r] + ex;
+        fu.row_nz[r] = ex < 0 ? 0 : cnt;
+        if (ex < 0) dev_report(st, kDevTimeout, 16, r);
+      }
+    }
+    __syncthreads();
+    return s_off;
+  };
+  // rows this form does not take: fused ones are counted here (a hash over
+  // the shared arena) and published; all go to the radix-sort ESC kernel
+  auto defer = [&]() {
+    if (FUSED) {
+      uint32_t* tab = skey;
+      __syncthreads();
+      for (int i = threadIdx.x; i < TS; i += BLOCK) tab[i] = kEmptyKey;
+      __syncthreads();
+      int cnt = 0;
+      for (int64_t a0 = as; a0 < ae; a0 += ACH) {
+        const int na = (int)((ae - a0) < (int64_t)ACH ? (ae - a0) : (int64_t)ACH);
+        const int t = stage_chunk<BLOCK, false, VIn>(A, B, a0, na, sg, segof, CAP, false);
+        expand_chunk<BLOCK, false, VIn>(B, t, sg, segof, [&](int32_t key, VIn, VIn, int) {
+          uint32_t h = hash_slot((uint32_t)key, TB);
+          for (int probe = 0; probe < TS; ++probe) {
+            const uint32_t old = atomicCAS(&tab[h], kEmptyKey, (uint32_t)key);
+            if (old == kEmptyKey) { ++cnt; return; }
+            if (old == (uint32_t)key) return;
+            h = (h + 1) & (TS - 1);
+          }
+        });
+        __syncthreads();
+      }
+      place(block_sum<BLOCK, int>(cnt, sg.tmp));
+    }
+    if (threadIdx.x == 0) ovf[atomicAdd(ovf_count, 1u)] = (int32_t)r;
+  };
+  if (ae - as > ACH) {  // uniform: more than one staged chunk
+    defer();
+    return;
+  }
+  if (threadIdx.x == 0) {
+    sg.kmin = b_sorted ? 0xFFFFFFFFu : 0u;
+    sg.kmax = b_sorted ? 0u : (uint32_t)(B.ncol > 0 ? B.ncol - 1 : 0);
+    sg.over = 0;
+  }
+  for (int i = threadIdx.x; i < NB / 2; i += BLOCK) bcnt[i] = 0u;
+  __syncthreads();
+  const int n = stage_chunk<BLOCK, true, VIn>(A, B, as, (int)(ae - as), sg, segof, CAP, b_sorted != 0);
+  if (n > CAP) {  // uniform: the bin bound was violated
+    if (threadIdx.x == 0) dev_report(st, kDevCapacity, 16, r);
+    if (FUSED) place(0);
+    return;
+  }
+  const uint32_t lo = sg.kmin;
+  const int bits = (sg.kmax > sg.kmin) ? 32 - __clz(sg.kmax - sg.kmin) : 0;
+  const int shift = bits > NBB ? bits - NBB : 0;
+  // pass 1: keys only, bucket histogram
+  int huge;
+  expand_chunk<BLOCK, false, VIn>(B, n, sg, segof, [&](int32_t key, VIn, VIn, int) {
+    bucket_add(bcnt, (int)(((uint32_t)key - lo) >> shift));
+  });
+  __syncthreads();
+  // exclusive scan of the bucket counts: NB / BLOCK consecutive buckets per thread
+  constexpr int WPT = NB / (2 * BLOCK);
+  {
+    uint32_t loc[WPT];
+    uint32_t sum = 0;
+    int nh = 0;  // buckets of more than kBucketLimit pairs
+#pragma unroll
+    for (int i = 0; i < WPT; ++i) {
+      loc[i] = bcnt[threadIdx.x * WPT + i];
+      const uint32_t c0 = loc[i] & 0xFFFFu, c1 = loc[i] >> 16;
+      sum += c0 + c1;
+      nh += (c0 > (uint32_t)kBucketLimit) + (c1 > (uint32_t)kBucketLimit);
+    }
+    // at most one huge bucket, over at most kHugeWidth columns, in this form
+    huge = __syncthreads_count(nh > 0);
+    if (__syncthreads_or(nh > 1 || (nh > 0 && (1 << shift) > kHugeWidth)) || huge > 1) {
+      defer();
+      return;
+    }
+    int tot_all;
+    uint32_t run = (uint32_t)block_exclusive_sum<BLOCK, int>((int)sum, sg.tmp, tot_all);
+#pragma unroll
+    for (int i = 0; i < WPT; ++i) {
+      const uint32_t c0 = loc[i] & 0xFFFFu, c1 = loc[i] >> 16;
+      bcnt[threadIdx.x * WPT + i] = run | ((run + c0) << 16);
+      run += c0 + c1;
+    }
+  }
+  __syncthreads();
+  // pass 2: (column, product index) into bucket order
+  expand_chunk<BLOCK, false, VIn>(B, n, sg, segof, [&](int32_t key, VIn, VIn, int p) {
+    const int pos = (int)bucket_add(bcnt, (int)(((uint32_t)key - lo) >> shift));
+    skey[pos] = (uint32_t)key;
+    sidx[pos] = (uint16_t)p;
+  });
+  __syncthreads();
+  // sort each bucket: a lane per bucket of 2..8 pairs (one network size per
+  // warp), then the warp's buckets of 9..kBucketLimit pairs one at a time;
+  // a bucket of more pairs over at most kHugeWidth columns (hub columns) is
+  // left to the whole block
+  for (int g = warp; g < NG; g += NW) {
+    const int b = g * 32 + lane;
+    const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
+    if (e - s > kBucketLimit) s_huge = b;
+    const int small = (e - s <= 8) ? e - s : 0;
+    const int mx = __reduce_max_sync(kFull, small);
+    if (small > 1) {
+      const uint32_t kbase = lo + ((uint32_t)b << shift);
+      if (mx <= 4) sort_perm_small<4>(skey, sidx, s, e, kbase);
+      else if (mx <= 6) sort_perm_small<6>(skey, sidx, s, e, kbase);
+      else sort_perm_small<8>(skey, sidx, s, e, kbase);
+    }
+    for (unsigned bigm = __ballot_sync(kFull, e - s > 8 && e - s <= kBucketLimit); bigm; bigm &= bigm - 1) {
+      const int l = __ffs(bigm) - 1;
+      warp_sort_perm(skey, sidx, __shfl_sync(kFull, s, l), __shfl_sync(kFull, e, l));
+    }
+  }
+  __syncthreads();
+  if (huge) {
+    // sums by column offset in hsum, then the bucket's slots become its
+    // present columns in order (product index kFromSum: the value is the
+    // sum) followed by fillers repeating the last column (kNoProduct: no
+    // value), so the runs and heads below see one slot per column
+    const int b = s_huge;
+    const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
+    const int width = 1 << shift;
+    const uint32_t kb = lo + ((uint32_t)b << shift);
+    for (int j = threadIdx.x; j < width; j += BLOCK) hsum[j] = AT(0);
+    if (threadIdx.x < kHugeWidth / 32) hmask[threadIdx.x] = 0u;
+    if (threadIdx.x == 0) s_hkb = kb;
+    __syncthreads();
+    for (int i = s + threadIdx.x; i < e; i += BLOCK) {
+      const int off = (int)(skey[i] - kb);
+      atomic_add_sh(&hsum[off], slot_value(sidx[i]));
+      atomicOr(&hmask[off >> 5], 1u << (off & 31));
+      place_of[sidx[i]] = kSkip;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int run = 0, lastc = 0;
+      for (int w = 0; w < kHugeWidth / 32; ++w) {
+        hpre[w] = run;
+        run += __popc(hmask[w]);
+        if (hmask[w]) lastc = w * 32 + 31 - __clz(hmask[w]);
+      }
+      hpre[kHugeWidth / 32] = run;
+      s_hlast = lastc;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < width; j += BLOCK) {
+      const uint32_t m = hmask[j >> 5];
+      if (m & (1u << (j & 31))) {
+        const int pos = s + hpre[j >> 5] + __popc(m & ((1u << (j & 31)) - 1u));
+        skey[pos] = kb + (uint32_t)j;
+        sidx[pos] = kFromSum;
+      }
+    }
+    for (int i = s + hpre[kHugeWidth / 32] + threadIdx.x; i < e; i += BLOCK) {
+      skey[i] = kb + (uint32_t)s_hlast;
+      sidx[i] = kNoProduct;
+    }
+    __syncthreads();
+  }
+  // run heads (first slot of each column) per 32-slot chunk, then offsets
+  const int nch = (n + 31) >> 5;
+  auto is_head = [&](int t) { return t < n && (t == 0 || skey[t] != skey[t - 1]); };
+  for (int c = warp; c < nch; c += NW) {
+    const unsigned m = __ballot_sync(kFull, is_head(c * 32 + lane));
+    if (lane == 0) ccnt[c] = __popc(m);
+  }
+  __syncthreads();
+  int distinct;
+  {
+    const int cnum = threadIdx.x < nch ? (int)ccnt[threadIdx.x] : 0;
+    const int ex = block_exclusive_sum<BLOCK, int>(cnum, sg.tmp, distinct);
+    if (threadIdx.x < nch) ccnt[threadIdx.x] = (uint32_t)ex;
+  }
+  __syncthreads();
+  int64_t c0, nz;
+  if (FUSED) {
+    c0 = place(distinct);
+    if (c0 < 0) return;
+    nz = distinct;
+    if (c0 + nz > fu.cap) {
+      if (threadIdx.x == 0) dev_report(st, kDevRowOverflow, 16, r);
+      return;
+    }
+  } else {
+    c0 = crp[r];
+    nz = crp[r + 1] - c0;
+  }
+  // sorted order: each distinct column to C, each product's place; a
+  // column of several products is zeroed for the atomic adds
+  for (int c = warp; c < nch; c += NW) {
+    const int t = c * 32 + lane;
+    const bool in = t < n;
+    const uint32_t key = in ? skey[t] : 0u;
+    const bool hd = in && (t == 0 || skey[t - 1] != key);
+    const bool last = in && (t + 1 == n || skey[t + 1] != key);
+    const unsigned m = __ballot_sync(kFull, hd);
+    const int run = (int)ccnt[c] + __popc(m & ((lanemask_lt() << 1) | 1u)) - 1;
+    if (in) {
+      const uint16_t p = sidx[t];
+      if (run >= nz) {  // more columns than the symbolic count (reported below)
+        if (p < kFromSum) place_of[p] = kSkip;
+      } else {
+        if (hd) ccol[c0 + run] = (int32_t)key;
+        if (p == kFromSum) {
+          cval[c0 + run] = hsum[key - s_hkb];
+        } else if (p != kNoProduct) {
+          const bool single = hd && last;
+          place_of[p] = (uint16_t)run | (single ? 0 : kShared);
+          if (hd && !single) cval[c0 + run] = AT(0);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // product order: a_ik * b_kj to its place
+  expand_values<BLOCK, VIn>(B, n, sg, segof, [&](VIn av, VIn bv, int p) {
+    const uint16_t o = place_of[p];
+    if (o == kSkip || (int)(o & ~kShared) >= nz) return;
+    const AT v = Acc<VIn>::mul(av, bv);
+    if (o & kShared) Acc<VIn>::atomic_add(&cval[c0 + (o & ~kShared)], v);
+    else cval[c0 + o] = v;
+  });
+  if (!FUSED && threadIdx.x == 0 && distinct != nz)
+    dev_report(st, distinct > nz ? kDevRowOverflow : kDevRowUnderflow, 16, r);
+}
+
 // Hash accumulator for rows with at most 2^TBITS / 2 distinct columns: linear
 // probing on 32-bit keys with the value summed by shared-memory atomics
 // (ams_hash_numc_krnl, src/ams/ams_utils.c:238-296, in shared memory), then

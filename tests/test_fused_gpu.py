@@ -1,7 +1,8 @@
 """GPU: the fused ESC rows (no symbolic pass, offsets by look-back).
 
 Rows of 2049..4800 products are counted, sorted and placed by one kernel in
-row order.  Checked bit for bit against the oracle and against the same
+row order, in its index form (column and product index in shared memory) or
+its column-and-value form.  Checked bit for bit against the oracle and against the same
 product with fusion off: uniform rows (nearly all fused), rows whose
 buckets overflow (deferred to the radix-sort kernel after an in-kernel
 count), int32 values, rows split over several A chunks, device output.
@@ -22,20 +23,21 @@ def same(out, ref):
     np.testing.assert_array_equal(out.csr.vals.astype(np.float64), ref[2])
 
 
-def hot_column_matrix(seed=3, ncol=3000):
-    """Rows whose products crowd one bucket: 160 A entries whose B rows all
-    hold column 0 (so 160 equal keys), plus other columns below ncol."""
+def hot_column_matrix(seed=3, ncol=3000, per_row=160, hot=1):
+    """Rows whose products crowd one bucket: per_row A entries whose B rows
+    all hold columns 0..hot-1 (so per_row * hot keys in the first bucket),
+    plus other columns below ncol, 20 per B row."""
     rng = np.random.default_rng(seed)
     n_rows, n_mid = 40, 400
     r, c = [], []
     for i in range(n_rows):
-        ks = rng.choice(n_mid, 160, replace=False)
-        r += [i] * 160
+        ks = rng.choice(n_mid, per_row, replace=False)
+        r += [i] * per_row
         c += list(ks)
     A = from_coo(n_rows, n_mid, np.array(r), np.array(c))
     br, bc = [], []
     for k in range(n_mid):
-        cols = np.concatenate([[0], rng.choice(np.arange(1, ncol), 19, replace=False)])
+        cols = np.concatenate([np.arange(hot), rng.choice(np.arange(hot, ncol), 20 - hot, replace=False)])
         br += [k] * 20
         bc += list(cols)
     B = from_coo(n_mid, ncol, np.array(br), np.array(bc))
@@ -70,18 +72,39 @@ def test_overflowing_fused_rows_are_deferred(ctx):
     same(out, ref)
 
 
-@pytest.mark.parametrize("fuse", [True, False])
-def test_huge_narrow_buckets_summed_densely(ctx, fuse):
-    # columns below 3000: the hot column's bucket spans 2 columns, summed by
-    # the whole block in place, no row deferred
-    A, B = hot_column_matrix()
+@pytest.mark.parametrize("fuse,form", [(True, 0), (False, 0), (True, 1)])
+def test_huge_narrow_buckets_summed_densely(ctx, fuse, form):
+    # columns below 3000: the hot columns' bucket spans 2 columns, summed by
+    # the whole block in place, no row deferred.  The index form takes rows
+    # of one staged chunk (at most 128 A entries): 120 entries, 2 hot columns
+    A, B = hot_column_matrix() if form == 0 else hot_column_matrix(per_row=120, hot=2)
     ref = oracle.oracle_spgemm(A, B, "hybacc")
-    ctx.set_fusion(fuse)
+    saved = ctx.get_tuning()
+    ctx.set_tuning(fusion=int(fuse), fused_form=form)
     try:
         out = ctx.spgemm(A, B, "hybacc")
     finally:
-        ctx.set_fusion(True)
+        ctx.set_tuning(**saved)
+    if fuse:
+        assert out.stats["fused_rows"] == A.num_row
     assert out.stats["esc_overflow_rows"] == 0
+    same(out, ref)
+
+
+def test_index_form_defers_two_huge_buckets(ctx):
+    # hot columns 0, 1 and 2048, 2049 over 4096 columns (buckets of 2
+    # columns): two buckets of 240 products each
+    rng = np.random.default_rng(5)
+    A, B = hot_column_matrix(per_row=120, hot=1, ncol=4096)
+    hot = [0, 1, 2048, 2049]
+    br, bc = np.repeat(np.arange(B.num_row), 20), []
+    for k in range(B.num_row):
+        bc.append(np.concatenate([hot, rng.choice(np.setdiff1d(np.arange(4096), hot), 16, replace=False)]))
+    B = from_coo(B.num_row, 4096, br, np.concatenate(bc))
+    ref = oracle.oracle_spgemm(A, B, "hybacc")
+    out = ctx.spgemm(A, B, "hybacc")
+    assert out.stats["fused_rows"] == A.num_row
+    assert out.stats["esc_overflow_rows"] == A.num_row
     same(out, ref)
 
 
@@ -105,9 +128,16 @@ def test_fused_rows_over_several_a_chunks(ctx):
     bc = np.concatenate([rng.choice(5000, 15, replace=False) for _ in range(1000)])
     B = from_coo(1000, 5000, br, bc, rng.integers(1, 5, len(br)).astype(np.float64))
     ref = oracle.oracle_spgemm(A, B, "hybacc")
-    out = ctx.spgemm(A, B, "hybacc")
-    assert out.stats["fused_rows"] == 30
-    same(out, ref)
+    saved = ctx.get_tuning()
+    try:
+        for form, deferred in ((1, 30), (0, 0)):  # the index form takes one staged chunk
+            ctx.set_tuning(fused_form=form)
+            out = ctx.spgemm(A, B, "hybacc")
+            assert out.stats["fused_rows"] == 30
+            assert out.stats["esc_overflow_rows"] == deferred
+            same(out, ref)
+    finally:
+        ctx.set_tuning(**saved)
 
 
 def test_fused_device_output_digest(ctx):
@@ -155,7 +185,7 @@ def test_tuning_routes_rows_but_not_results(ctx):
     seen = set()
     try:
         for kw in ({"esc_max_products": 1024}, {"hash_max_nnz": 256}, {"fused_min_products": 512},
-                   {"acc_thres": 5.0}, {"fusion": 0}):
+                   {"acc_thres": 5.0}, {"fusion": 0}, {"fused_form": 0}, {"fused_form": 0, "fused_min_products": 512}):
             ctx.set_tuning(**saved)
             ctx.set_tuning(**kw)
             out = ctx.spgemm(A, B, "hybacc")
