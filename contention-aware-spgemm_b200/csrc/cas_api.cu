@@ -67,7 +67,8 @@ struct cas_ctx {
   bool profile = false;
   bool fuse = true;                        // fused ESC rows (no symbolic pass) in cas_spgemm
   int fused_lo = (int)cas::kFusedLo;       // fused rows: more products than this (up to kFusedHi)
-  int fused_form = 1;                      // fused kernel: 1 index form (k_numc_esc_idx), 0 k_numc_esc_msd
+  int esc_form = 1;                        // bucketed ESC of rows over 4096 products (fused rows included):
+                                           // 1 index form (k_numc_esc_idx), 0 k_numc_esc_msd
   int esc_max = 8192;                      // ESC rows: at most this many products
   int hash_max = 4096;                     // hash rows: at most this many distinct columns
   double acc_thres = 2.0;
@@ -213,8 +214,9 @@ constexpr size_t smem_numc_esc_idx() {
 template <typename VIn>
 cas_status setup_numc_kernels(cas_ctx* ctx) {
   using namespace cas;
-#define CAS_SETUP_ESC(bin, CAP, NBB) \
-  CAS_TRY(allow_smem(ctx, k_numc_esc_msd<256, CAP, NBB, VIn>, smem_numc_esc_msd<CAP, NBB, VIn>()));
+#define CAS_SETUP_ESC(bin, CAP, NBB)                                                               \
+  CAS_TRY(allow_smem(ctx, k_numc_esc_msd<256, CAP, NBB, VIn>, smem_numc_esc_msd<CAP, NBB, VIn>())); \
+  if constexpr (CAP > 4096) CAS_TRY(allow_smem(ctx, k_numc_esc_idx<256, CAP, NBB, VIn>, smem_numc_esc_idx<CAP, NBB, VIn>()));
   CAS_ESC_SHAPES(CAS_SETUP_ESC)
 #undef CAS_SETUP_ESC
   CAS_TRY(allow_smem(ctx, k_numc_esc_msd<256, (int)kFusedHi, 11, VIn, true>,
@@ -668,7 +670,7 @@ cas_status launch_fused(cas_ctx* ctx, Call& c, const int64_t* known, int32_t* cc
   CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + kSlotFused + 4, 0, sizeof(unsigned long long), ctx->stream));
   Fused fu{c.frows, ctx->d_counts + kSlotFused + 4, c.fstatus, known, c.row_nz, cap};
   if (ctx->profile) CAS_CUDA(ctx, cudaEventRecord(ctx->ev_fused[0], ctx->stream));
-  if (ctx->fused_form == 1)
+  if (ctx->esc_form == 1)
     k_numc_esc_idx<256, (int)kFusedHi, 11, VIn, true>
         <<<(unsigned)c.nf, 256, smem_numc_esc_idx<(int)kFusedHi, 11, VIn>(), ctx->stream>>>(
             nullptr, c.A.csr, c.B.csr, c.b_sorted ? 1 : 0, nullptr, ccol, static_cast<AT*>(cval), c.ovf, ovf_count,
@@ -782,6 +784,24 @@ cas_status numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int mode) {
 }
 
 // ------------------------------------------------------------------ NUMC
+// One bucketed ESC bin: the index form for bins of more than 4096 products
+// when esc_form is 1, else the column-and-value form.
+template <int CAP, int NBB, typename VIn>
+void launch_esc_bin(int esc_form, int64_t n, cudaStream_t s, const int32_t* rows, const cas::Csr& A, const cas::Csr& B,
+                    int32_t b_sorted, const int64_t* crp, int32_t* ccol, typename cas::Acc<VIn>::T* cval, int32_t* ovf,
+                    unsigned int* ovf_count, cas::DevStatus* st) {
+  using namespace cas;
+  if constexpr (CAP > 4096) {
+    if (esc_form == 1) {
+      k_numc_esc_idx<256, CAP, NBB, VIn><<<(unsigned)n, 256, smem_numc_esc_idx<CAP, NBB, VIn>(), s>>>(
+          rows, A, B, b_sorted, crp, ccol, cval, ovf, ovf_count, st, Fused{});
+      return;
+    }
+  }
+  k_numc_esc_msd<256, CAP, NBB, VIn><<<(unsigned)n, 256, smem_numc_esc_msd<CAP, NBB, VIn>(), s>>>(
+      rows, A, B, b_sorted, crp, ccol, cval, ovf, ovf_count, st, Fused{});
+}
+
 template <typename VIn>
 cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* ccol, void* cval_v) {
   using namespace cas;
@@ -808,11 +828,11 @@ cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* 
       case kNB_Tiny:
         k_numc_tiny<256, VIn><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(rows, n, A, B, crp, ccol, cval, ctx->d_status);
         break;
-#define CAS_ESC_CASE(bin, CAP, NBB)                                                                     \
-      case bin:                                                                                         \
-        esc_rows += n;                                                                                  \
-        k_numc_esc_msd<256, CAP, NBB, VIn><<<(unsigned)n, 256, smem_numc_esc_msd<CAP, NBB, VIn>(), s>>>( \
-            rows, A, B, c.b_sorted ? 1 : 0, crp, ccol, cval, c.ovf, ovf_count, ctx->d_status, Fused{});  \
+#define CAS_ESC_CASE(bin, CAP, NBB)                                                                      \
+      case bin:                                                                                          \
+        esc_rows += n;                                                                                   \
+        launch_esc_bin<CAP, NBB, VIn>(ctx->esc_form, n, s, rows, A, B, c.b_sorted ? 1 : 0, crp, ccol, cval, \
+                                      c.ovf, ovf_count, ctx->d_status);                                  \
         break;
       CAS_ESC_SHAPES(CAS_ESC_CASE)
 #undef CAS_ESC_CASE
@@ -1144,14 +1164,14 @@ cas_status cas_set_tuning(cas_ctx* ctx, const cas_tuning* t) {
   if (!ctx || !t) return CAS_ERR_BAD_INPUT;
   if (!(t->acc_thres >= 0.0) || t->fused_min_products < 32 || t->fused_min_products >= (int)cas::kFusedHi ||
       t->esc_max_products < 32 || t->esc_max_products > 8192 || t->hash_max_nnz < 0 || t->hash_max_nnz > 4096 ||
-      (t->fused_form != 0 && t->fused_form != 1))
+      (t->esc_form != 0 && t->esc_form != 1))
     return set_err(ctx, CAS_ERR_BAD_INPUT, "tuning out of range");
   ctx->acc_thres = t->acc_thres;
   ctx->fuse = t->fusion != 0;
   ctx->fused_lo = t->fused_min_products;
   ctx->esc_max = t->esc_max_products;
   ctx->hash_max = t->hash_max_nnz;
-  ctx->fused_form = t->fused_form;
+  ctx->esc_form = t->esc_form;
   return CAS_OK;
 }
 
@@ -1162,7 +1182,7 @@ cas_status cas_get_tuning(const cas_ctx* ctx, cas_tuning* t) {
   t->fused_min_products = ctx->fused_lo;
   t->esc_max_products = ctx->esc_max;
   t->hash_max_nnz = ctx->hash_max;
-  t->fused_form = ctx->fused_form;
+  t->esc_form = ctx->esc_form;
   return CAS_OK;
 }
 

@@ -141,9 +141,10 @@ typedef struct {
 	int32_t esc_max_products;    /* ESC rows have at most this many products, <= 8192 [8192] */
 	int32_t hash_max_nnz;        /* hash rows have at most this many distinct columns, <= 4096 [4096];
 	                                larger rows take the dense kernels */
-	int32_t fused_form;          /* kernel of the fused rows: 1 keeps a column and a product index per
-	                                product in shared memory, 4 rows per SM [1]; 0 keeps column and
-	                                value, 3 rows per SM */
+	int32_t esc_form;            /* bucketed ESC kernel of the fused rows and of ESC rows over 4096
+	                                products: 1 keeps column, product index and place per product in
+	                                shared memory, 4 rows per SM [1]; 0 keeps column and value,
+	                                3 rows per SM */
 } cas_tuning;
 cas_status cas_set_tuning(cas_ctx *ctx, const cas_tuning *t);
 cas_status cas_get_tuning(const cas_ctx *ctx, cas_tuning *t);

@@ -80,7 +80,7 @@ def test_huge_narrow_buckets_summed_densely(ctx, fuse, form):
     A, B = hot_column_matrix() if form == 0 else hot_column_matrix(per_row=120, hot=2)
     ref = oracle.oracle_spgemm(A, B, "hybacc")
     saved = ctx.get_tuning()
-    ctx.set_tuning(fusion=int(fuse), fused_form=form)
+    ctx.set_tuning(fusion=int(fuse), esc_form=form)
     try:
         out = ctx.spgemm(A, B, "hybacc")
     finally:
@@ -131,7 +131,7 @@ def test_fused_rows_over_several_a_chunks(ctx):
     saved = ctx.get_tuning()
     try:
         for form, deferred in ((1, 30), (0, 0)):  # the index form takes one staged chunk
-            ctx.set_tuning(fused_form=form)
+            ctx.set_tuning(esc_form=form)
             out = ctx.spgemm(A, B, "hybacc")
             assert out.stats["fused_rows"] == 30
             assert out.stats["esc_overflow_rows"] == deferred
@@ -185,7 +185,7 @@ def test_tuning_routes_rows_but_not_results(ctx):
     seen = set()
     try:
         for kw in ({"esc_max_products": 1024}, {"hash_max_nnz": 256}, {"fused_min_products": 512},
-                   {"acc_thres": 5.0}, {"fusion": 0}, {"fused_form": 0}, {"fused_form": 0, "fused_min_products": 512}):
+                   {"acc_thres": 5.0}, {"fusion": 0}, {"esc_form": 0}, {"esc_form": 0, "fused_min_products": 512}):
             ctx.set_tuning(**saved)
             ctx.set_tuning(**kw)
             out = ctx.spgemm(A, B, "hybacc")
