@@ -526,12 +526,15 @@ def main():
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9 if dom_ms > 0 else 0.0
     kernel_name = {"tiny": "k_numc_tiny<256>", "hash256": "k_numc_hash<256,9>", "hash1k": "k_numc_hash<256,11>",
                    "hash4k": "k_numc_hash<512,13>", "dense": "k_numc_dense<512>"}.get(dom)
+    # the index form runs the fused rows and the ESC bins over 4096 products when esc_form is 1
+    idx_form = ctx.get_tuning().get("esc_form", 1) == 1
     if dom == "fused":
-        kernel_name = "k_numc_esc_msd<256,4800,11,fused>"
+        kernel_name = "k_numc_esc_%s<256,4800,11,fused>" % ("idx" if idx_form else "msd")
     if kernel_name is None and dom.startswith("esc"):
-        kernel_name = "k_numc_esc_msd<256,%s>" % {"esc1k": "1024,9", "esc2k": "2048,9", "esc3k": "3072,10",
-                                                   "esc4k": "4096,10", "esc5k": "4800,11", "esc6k": "6144,11",
-                                                   "esc8k": "8192,11"}[dom]
+        shape = {"esc1k": "1024,9", "esc2k": "2048,9", "esc3k": "3072,10", "esc4k": "4096,10",
+                 "esc5k": "4800,11", "esc6k": "6144,11", "esc8k": "8192,11"}[dom]
+        big = dom in ("esc5k", "esc6k", "esc8k")
+        kernel_name = "k_numc_esc_%s<256,%s>" % ("idx" if idx_form and big else "msd", shape)
     alg_bytes_total = 12.0 * (A.nnz if world == 1 else As.nnz) + 12.0 * P_local + 12.0 * nnz_local + 16.0 * (As.num_row + 1)
     pipe_frac = alg_bytes_total / (ms_step * 1e-3) / (peak * 1e9)
 
