@@ -182,10 +182,10 @@ constexpr size_t smem_numc_esc_msd() {
          ((size_t(CAP) + 15) & ~size_t(15)) + sizeof(cas::StageB<VIn>);
 }
 
-// index form: column, product index and place per product, padded chunk counts
+// index form: column, product index and place per product, padded chunk counts and head masks
 template <int CAP, int NBB, typename VIn>
 constexpr size_t smem_numc_esc_idx() {
-  return size_t(CAP) * 8 + (size_t(1) << NBB) * 2 + size_t((CAP / 32 + 3) & ~3) * 4 +
+  return size_t(CAP) * 8 + (size_t(1) << NBB) * 2 + size_t((CAP / 32 + 3) & ~3) * 8 +
          ((size_t(CAP) + 15) & ~size_t(15)) + sizeof(cas::StageB<VIn>);
 }
 

@@ -1017,6 +1017,40 @@ __device__ long long lookback_prefix(unsigned long long* status, int64_t t, long
   return excl;
 }
 
+// The two halves of lookback_prefix, for a block that has other work between
+// them: one thread publishes the row's count (ticket 0: its inclusive
+// prefix) ...
+__device__ __forceinline__ void lookback_publish(unsigned long long* status, int64_t t, long long count) {
+  st_release_u64(&status[t], (t == 0 ? kLbInc : kLbAgg) | (unsigned long long)count);
+}
+
+// ... and later warp 0 sums the counts of all earlier tickets, publishes the
+// inclusive prefix and returns the exclusive one (-1 when a wait gave up).
+__device__ long long lookback_resolve(unsigned long long* status, int64_t t, long long count) {
+  const int lane = threadIdx.x & 31;
+  if (t == 0) return 0;
+  long long excl = 0;
+  int64_t j = t - 1;
+  int spins = 0;
+  for (;;) {
+    const int64_t idx = j - lane;
+    const unsigned long long v = idx >= 0 ? ld_acquire_u64(&status[idx]) : kLbInc;
+    if (__any_sync(kFull, (v >> 62) == 0)) {
+      if (++spins > kLbSpins) return -1;
+      __nanosleep(64);
+      continue;
+    }
+    const unsigned inc = __ballot_sync(kFull, (v >> 62) == 2);
+    const int stop = inc ? __ffs(inc) - 1 : 31;
+    long long part = lane <= stop ? (long long)(v & kLbVal) : 0;
+    excl += warp_sum(part);
+    if (inc) break;
+    j -= 32;
+  }
+  if (lane == 0) st_release_u64(&status[t], kLbInc | (unsigned long long)(excl + count));
+  return excl;
+}
+
 __host__ __device__ constexpr int floor_pow2(int x) { return x < 2 ? 1 : 2 * floor_pow2(x / 2); }
 
 template <int BLOCK, int CAP, int NBB, typename VIn, bool FUSED = false>
@@ -1437,8 +1471,8 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   constexpr int NCH = CAP / 32;
   constexpr int NCHP = (NCH + 3) & ~3;  // chunk counts padded to 16 bytes
   constexpr int ACH = BLOCK < kBChunk ? BLOCK : kBChunk;
-  // the hash of deferred rows spans columns, indices, places, bucket and chunk counts
-  constexpr int TS = floor_pow2((CAP * 8 + NB * 2 + NCHP * 4) / 4);
+  // the hash of deferred rows spans columns, indices, places, bucket counts, chunk counts and masks
+  constexpr int TS = floor_pow2((CAP * 8 + NB * 2 + NCHP * 8) / 4);
   constexpr int TB = __builtin_ctz(TS);
   static_assert(CAP < 32768 && CAP % 32 == 0, "16-bit counters, product indices and places");
   static_assert(NG <= BLOCK && NCH <= BLOCK && NB % (2 * BLOCK) == 0, "one count per thread in the scans");
@@ -1449,7 +1483,8 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   uint16_t* place_of = sidx + CAP;                             // per product: its column's place in the row
   uint32_t* bcnt = reinterpret_cast<uint32_t*>(place_of + CAP);  // NB 16-bit counters
   uint32_t* ccnt = bcnt + NB / 2;                              // NCH head counts / offsets
-  uint8_t* segof = reinterpret_cast<uint8_t*>(ccnt + NCHP);
+  uint32_t* hmw = ccnt + NCHP;                                 // NCH head masks
+  uint8_t* segof = reinterpret_cast<uint8_t*>(hmw + NCHP);
   StageB<VIn>& sg = *reinterpret_cast<StageB<VIn>*>(segof + ((CAP + 15) & ~15));
   __shared__ long long s_tick, s_off;
   __shared__ int s_huge, s_hlast;
@@ -1654,7 +1689,10 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   auto is_head = [&](int t) { return t < n && (t == 0 || skey[t] != skey[t - 1]); };
   for (int c = warp; c < nch; c += NW) {
     const unsigned m = __ballot_sync(kFull, is_head(c * 32 + lane));
-    if (lane == 0) ccnt[c] = __popc(m);
+    if (lane == 0) {
+      ccnt[c] = __popc(m);
+      hmw[c] = m;
+    }
   }
   __syncthreads();
   int distinct;
@@ -1664,42 +1702,58 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
     if (threadIdx.x < nch) ccnt[threadIdx.x] = (uint32_t)ex;
   }
   __syncthreads();
-  int64_t c0, nz;
+  // fused rows: the count goes out now, the look-back waits until the
+  // places below are recorded, so the wait for earlier rows overlaps them
+  if (FUSED && threadIdx.x == 0) lookback_publish(fu.status, tick, distinct);
+  const int64_t nz = FUSED ? (int64_t)distinct : crp[r + 1] - crp[r];
+  auto head_at = [&](int t) -> bool { return t < n && ((hmw[t >> 5] >> (t & 31)) & 1u); };
+  // each product's place: the run of its column, flagged when the run has
+  // several products (those add into C atomically)
+  for (int c = warp; c < nch; c += NW) {
+    const int t = c * 32 + lane;
+    const unsigned m = hmw[c];
+    if (t < n) {
+      const uint16_t p = sidx[t];
+      const int run = (int)ccnt[c] + __popc(m & ((lanemask_lt() << 1) | 1u)) - 1;
+      if (p < kFromSum) {
+        const bool single = ((m >> lane) & 1u) && (t + 1 == n || head_at(t + 1));
+        place_of[p] = run >= nz ? kSkip : (uint16_t)run | (single ? 0 : kShared);
+      }
+    }
+  }
+  int64_t c0;
   if (FUSED) {
-    c0 = place(distinct);
+    if (warp == 0) {
+      const long long ex = lookback_resolve(fu.status, tick, distinct);
+      if (lane == 0) {
+        s_off = ex < 0 ? -1 : (long long)fu.known[r] + ex;
+        fu.row_nz[r] = ex < 0 ? 0 : distinct;
+        if (ex < 0) dev_report(st, kDevTimeout, 16, r);
+      }
+    }
+    __syncthreads();
+    c0 = s_off;
     if (c0 < 0) return;
-    nz = distinct;
     if (c0 + nz > fu.cap) {
       if (threadIdx.x == 0) dev_report(st, kDevRowOverflow, 16, r);
       return;
     }
   } else {
     c0 = crp[r];
-    nz = crp[r + 1] - c0;
+    __syncthreads();
   }
-  // sorted order: each distinct column to C, each product's place; a
-  // column of several products is zeroed for the atomic adds
+  // sorted order: each distinct column to C; the huge bucket's sums; a zero
+  // where several products will add
   for (int c = warp; c < nch; c += NW) {
     const int t = c * 32 + lane;
-    const bool in = t < n;
-    const uint32_t key = in ? skey[t] : 0u;
-    const bool hd = in && (t == 0 || skey[t - 1] != key);
-    const bool last = in && (t + 1 == n || skey[t + 1] != key);
-    const unsigned m = __ballot_sync(kFull, hd);
-    const int run = (int)ccnt[c] + __popc(m & ((lanemask_lt() << 1) | 1u)) - 1;
-    if (in) {
-      const uint16_t p = sidx[t];
-      if (run >= nz) {  // more columns than the symbolic count (reported below)
-        if (p < kFromSum) place_of[p] = kSkip;
-      } else {
-        if (hd) ccol[c0 + run] = (int32_t)key;
-        if (p == kFromSum) {
-          cval[c0 + run] = hsum[key - s_hkb];
-        } else if (p != kNoProduct) {
-          const bool single = hd && last;
-          place_of[p] = (uint16_t)run | (single ? 0 : kShared);
-          if (hd && !single) cval[c0 + run] = AT(0);
-        }
+    const unsigned m = hmw[c];
+    if ((m >> lane) & 1u) {
+      const int run = (int)ccnt[c] + __popc(m & lanemask_lt());
+      if (run < nz) {
+        const uint32_t key = skey[t];
+        ccol[c0 + run] = (int32_t)key;
+        if (sidx[t] == kFromSum) cval[c0 + run] = hsum[key - s_hkb];
+        else if (t + 1 < n && !head_at(t + 1) && sidx[t + 1] != kNoProduct) cval[c0 + run] = AT(0);
       }
     }
   }
@@ -1707,7 +1761,7 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   // product order: a_ik * b_kj to its place
   expand_values<BLOCK, VIn>(B, n, sg, segof, [&](VIn av, VIn bv, int p) {
     const uint16_t o = place_of[p];
-    if (o == kSkip || (int)(o & ~kShared) >= nz) return;
+    if (o == kSkip) return;
     const AT v = Acc<VIn>::mul(av, bv);
     if (o & kShared) Acc<VIn>::atomic_add(&cval[c0 + (o & ~kShared)], v);
     else cval[c0 + o] = v;
