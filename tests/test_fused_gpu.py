@@ -222,3 +222,30 @@ def test_autotuner_caches_per_class(ctx, tmp_path):
         same(out, oracle.oracle_spgemm(A, A.transpose(), "hybacc"))
     finally:
         ctx.set_tuning(**before)
+
+
+@pytest.mark.parametrize("per_b", [100, 180])
+def test_index_form_many_shared_columns(ctx, per_b):
+    """Rows of 3000 (fused) or 5400 (ESC bin) products of which half fall
+    on 300 common columns: hundreds of columns with several products each,
+    which the index form zeroes in C and adds into with global atomics."""
+    rng = np.random.default_rng(11)
+    n_rows, n_mid, ncol = 64, 600, 5000
+    r = np.repeat(np.arange(n_rows), 30)
+    c = np.concatenate([rng.choice(n_mid, 30, replace=False) for _ in range(n_rows)])
+    A = from_coo(n_rows, n_mid, r, c, rng.integers(1, 4, len(r)).astype(np.float64))
+    common = rng.choice(ncol, 300, replace=False)
+    br = np.repeat(np.arange(n_mid), per_b)
+    bc = np.concatenate([rng.choice(common, per_b, replace=False) if k % 2 else
+                         rng.choice(ncol, per_b, replace=False) for k in range(n_mid)])
+    B = from_coo(n_mid, ncol, br, bc, rng.integers(1, 4, len(br)).astype(np.float64))
+    ref = oracle.oracle_spgemm(A, B, "hybacc")
+    saved = ctx.get_tuning()
+    try:
+        for form in (1, 0):
+            ctx.set_tuning(esc_form=form)
+            out = ctx.spgemm(A, B, "hybacc")
+            assert out.stats["esc_overflow_rows"] == 0
+            same(out, ref)
+    finally:
+        ctx.set_tuning(**saved)
