@@ -591,7 +591,7 @@ def main():
             if it > 0:
                 walls.append(time.perf_counter() - tw)
             s = ctx.stats()
-            h2d, d2h = s["h2d_bytes"], s["d2h_bytes"]
+            h2d, d2h, d2h_direct = s["h2d_bytes"], s["d2h_bytes"], s["d2h_direct_bytes"]
             ctx.lib.cas_csr_free(ctx.h, ctypes.byref(cc))
         wall = statistics.mean(walls)
         if dist:
@@ -601,9 +601,10 @@ def main():
         line["e2e"] = {"value": round(2.0 * P_total / wall / 1e9, 3), "unit": "GFLOP/s",
                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                        "steps": args.e2e_steps, "s_per_step": round(wall, 3),
-                       "warmup": 1,
+                       "warmup": 1, "d2h_direct_bytes_per_step": d2h_direct,
                        "path": "cas_spgemm on pinned host A, B; C returned in host memory (after one untimed "
-                               "call, so C's host blocks are the context's resident ones)"}
+                               "call, so C's host blocks are the context's resident ones, registered with "
+                               "CUDA when they came back; d2h_direct bytes went to them by DMA directly)"}
         del hA, hB
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

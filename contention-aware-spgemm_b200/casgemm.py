@@ -56,7 +56,7 @@ class CasStats(ctypes.Structure):
         ("numc_bin_bytes", ctypes.c_double * 13), ("numc_bin_flop", ctypes.c_int64 * 13),
         ("esc_overflow_rows", ctypes.c_int64), ("esc_overflow_ms", ctypes.c_double),
         ("fused_rows", ctypes.c_int64), ("fused_flop", ctypes.c_int64), ("fused_bytes", ctypes.c_double),
-        ("fused_ms", ctypes.c_double),
+        ("fused_ms", ctypes.c_double), ("d2h_direct_bytes", ctypes.c_double),
     ]
 
 
@@ -309,7 +309,7 @@ class Context:
             "numc_bin_flop": dict(zip(NUMC_BINS, list(s.numc_bin_flop))),
             "esc_overflow_rows": s.esc_overflow_rows, "esc_overflow_ms": s.esc_overflow_ms,
             "fused_rows": s.fused_rows, "fused_flop": s.fused_flop, "fused_bytes": s.fused_bytes,
-            "fused_ms": s.fused_ms,
+            "fused_ms": s.fused_ms, "d2h_direct_bytes": s.d2h_direct_bytes,
         }
 
     def spgemm(self, A, B, accum: str = "hybacc", col_bytes: int = 4) -> Result:

@@ -21,6 +21,7 @@
 #include <mutex>
 #include <thread>
 #include <unordered_map>
+#include <unordered_set>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -86,6 +87,11 @@ struct cas_ctx {
   // context allocated, and the released ones kept for reuse
   std::unordered_map<void*, size_t> host_blocks;
   std::vector<std::pair<void*, size_t>> host_free;
+  // cached blocks registered with CUDA, which copies into them by DMA
+  // directly; registration is turned off after it fails once
+  std::unordered_set<void*> host_pinned;
+  bool host_pin_off = false;
+  double d2h_direct = 0;  // bytes the current call copied into registered blocks
   size_t host_free_bytes = 0;
 };
 
@@ -315,6 +321,27 @@ void* host_take(cas_ctx* ctx, size_t bytes) {
   return p;
 }
 
+// A block the cache keeps (at least kPinMin bytes) is registered with CUDA
+// when it enters the cache, once: a later output in it is copied from the
+// device by DMA directly, without the staging buffers.  The cost of
+// registering falls on the cas_csr_free that returns the block.
+constexpr size_t kPinMin = size_t(64) << 20;
+
+void host_pin(cas_ctx* ctx, void* p, size_t bytes) {
+  if (ctx->host_pin_off || bytes < kPinMin || ctx->host_pinned.count(p)) return;
+  constexpr size_t kHuge = size_t(2) << 20;  // the allocation's length, as host_alloc_huge rounds it
+  if (cudaHostRegister(p, (bytes + kHuge - 1) / kHuge * kHuge, cudaHostRegisterDefault) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->host_pin_off = true;
+    return;
+  }
+  ctx->host_pinned.insert(p);
+}
+
+void host_unpin(cas_ctx* ctx, void* p) {
+  if (ctx->host_pinned.erase(p)) cudaHostUnregister(p);
+}
+
 void host_give(cas_ctx* ctx, void* p) {
   if (!p) return;
   auto it = ctx ? ctx->host_blocks.find(p) : decltype(ctx->host_blocks)::iterator();
@@ -324,10 +351,12 @@ void host_give(cas_ctx* ctx, void* p) {
   }
   static const double phys = (double)sysconf(_SC_PHYS_PAGES) * (double)sysconf(_SC_PAGESIZE);
   if ((double)(ctx->host_free_bytes + it->second) > kHostCacheShare * phys) {
+    host_unpin(ctx, p);
     ctx->host_blocks.erase(it);
     free(p);
     return;
   }
+  host_pin(ctx, p, it->second);
   ctx->host_free.emplace_back(p, it->second);
   ctx->host_free_bytes += it->second;
 }
@@ -417,6 +446,17 @@ cas_status d2h_staged(cas_ctx* ctx, void* dst, const void* src, size_t bytes, bo
     }
   }
   return CAS_OK;
+}
+
+// Device -> host copy of one output array: by DMA straight into a block the
+// context has registered, else through the staging buffers.
+cas_status d2h_out(cas_ctx* ctx, void* dst, const void* src, size_t bytes, bool widen = false) {
+  if (bytes > 0 && !widen && ctx->host_pinned.count(dst)) {
+    CAS_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->d2h_direct += (double)bytes;
+    return CAS_OK;
+  }
+  return d2h_staged(ctx, dst, src, bytes, widen);
 }
 
 cas_status basic_checks(cas_ctx* ctx, const cas_csr* M, const char* name) {
@@ -896,6 +936,7 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
   using namespace cas;
   Call c;
   double h2d = 0, d2h = 0;
+  ctx->d2h_direct = 0;
   const bool c_on_device = C->on_device != 0;
   const int c_col_bytes = c_on_device ? 4 : (C->col_bytes == 8 ? 8 : 4);
   CAS_TRY(prepare(ctx, A, B, c, h2d));
@@ -995,9 +1036,9 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
     C->row_ptrs = h_rp;
     C->cols = h_col;
     C->rats = h_val;
-    CAS_TRY(d2h_staged(ctx, C->row_ptrs, crp, sizeof(int64_t) * (c.m + 1)));
-    CAS_TRY(d2h_staged(ctx, C->rats, cval, vbytes * nnz));
-    CAS_TRY(d2h_staged(ctx, C->cols, ccol, sizeof(int32_t) * nnz, c_col_bytes == 8));
+    CAS_TRY(d2h_out(ctx, C->row_ptrs, crp, sizeof(int64_t) * (c.m + 1)));
+    CAS_TRY(d2h_out(ctx, C->rats, cval, vbytes * nnz));
+    CAS_TRY(d2h_out(ctx, C->cols, ccol, sizeof(int32_t) * nnz, c_col_bytes == 8));
     d2h += sizeof(int64_t) * (double)(c.m + 1) + (vbytes + c_col_bytes) * (double)nnz;
     CAS_CUDA(ctx, cudaFreeAsync(crp, ctx->stream));
     CAS_CUDA(ctx, cudaFreeAsync(ccol, ctx->stream));
@@ -1022,6 +1063,7 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
   s.kernel_launches = ctx->launches;
   s.h2d_bytes = h2d;
   s.d2h_bytes = d2h;
+  s.d2h_direct_bytes = ctx->d2h_direct;
   const double vin = c.vt == CAS_VAL_F64 ? 8.0 : 4.0;
   for (int b = 0; b < kNumcBins; ++b) {
     const double flp = (double)ctx->h_counts[kSlotBinSums + b];
@@ -1141,6 +1183,8 @@ void cas_destroy(cas_ctx* ctx) {
     if (ctx->h_stage[i]) cudaFreeHost(ctx->h_stage[i]);
     if (ctx->ev_stage[i]) cudaEventDestroy(ctx->ev_stage[i]);
   }
+  // blocks still held by callers stay valid host memory, no longer registered
+  for (void* p : ctx->host_pinned) cudaHostUnregister(p);
   for (auto& b : ctx->host_free) free(b.first);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;

@@ -105,6 +105,9 @@ typedef struct {
 	int64_t fused_flop;
 	double fused_bytes;
 	double fused_ms;
+	/* of d2h_bytes, those copied by DMA straight into host blocks the
+	 * context has registered (blocks it kept from earlier outputs) */
+	double d2h_direct_bytes;
 } cas_stats;
 
 typedef struct cas_ctx cas_ctx;
