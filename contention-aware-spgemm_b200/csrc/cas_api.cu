@@ -18,6 +18,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -325,21 +326,40 @@ void* host_take(cas_ctx* ctx, size_t bytes) {
 // when it enters the cache, once: a later output in it is copied from the
 // device by DMA directly, without the staging buffers.  The cost of
 // registering falls on the cas_csr_free that returns the block.
+// Registered memory cannot be paged out, so all contexts of the process
+// together register at most kPinShare of physical memory; past that, blocks
+// stay unregistered and their outputs go through staging.
 constexpr size_t kPinMin = size_t(64) << 20;
+constexpr double kPinShare = 0.6;
+std::atomic<size_t> g_pinned_bytes{0};
+
+size_t pin_length(size_t bytes) {
+  constexpr size_t kHuge = size_t(2) << 20;  // the allocation's length, as host_alloc_huge rounds it
+  return (bytes + kHuge - 1) / kHuge * kHuge;
+}
 
 void host_pin(cas_ctx* ctx, void* p, size_t bytes) {
   if (ctx->host_pin_off || bytes < kPinMin || ctx->host_pinned.count(p)) return;
-  constexpr size_t kHuge = size_t(2) << 20;  // the allocation's length, as host_alloc_huge rounds it
-  if (cudaHostRegister(p, (bytes + kHuge - 1) / kHuge * kHuge, cudaHostRegisterDefault) != cudaSuccess) {
+  static const double phys = (double)sysconf(_SC_PHYS_PAGES) * (double)sysconf(_SC_PAGESIZE);
+  const size_t len = pin_length(bytes);
+  if ((double)(g_pinned_bytes.fetch_add(len) + len) > kPinShare * phys) {
+    g_pinned_bytes.fetch_sub(len);
+    return;
+  }
+  if (cudaHostRegister(p, len, cudaHostRegisterDefault) != cudaSuccess) {
     cudaGetLastError();
+    g_pinned_bytes.fetch_sub(len);
     ctx->host_pin_off = true;
     return;
   }
   ctx->host_pinned.insert(p);
 }
 
-void host_unpin(cas_ctx* ctx, void* p) {
-  if (ctx->host_pinned.erase(p)) cudaHostUnregister(p);
+void host_unpin(cas_ctx* ctx, void* p, size_t bytes) {
+  if (ctx->host_pinned.erase(p)) {
+    cudaHostUnregister(p);
+    g_pinned_bytes.fetch_sub(pin_length(bytes));
+  }
 }
 
 void host_give(cas_ctx* ctx, void* p) {
@@ -351,7 +371,7 @@ void host_give(cas_ctx* ctx, void* p) {
   }
   static const double phys = (double)sysconf(_SC_PHYS_PAGES) * (double)sysconf(_SC_PAGESIZE);
   if ((double)(ctx->host_free_bytes + it->second) > kHostCacheShare * phys) {
-    host_unpin(ctx, p);
+    host_unpin(ctx, p, it->second);
     ctx->host_blocks.erase(it);
     free(p);
     return;
@@ -1184,7 +1204,10 @@ void cas_destroy(cas_ctx* ctx) {
     if (ctx->ev_stage[i]) cudaEventDestroy(ctx->ev_stage[i]);
   }
   // blocks still held by callers stay valid host memory, no longer registered
-  for (void* p : ctx->host_pinned) cudaHostUnregister(p);
+  for (void* p : ctx->host_pinned) {
+    cudaHostUnregister(p);
+    g_pinned_bytes.fetch_sub(pin_length(ctx->host_blocks[p]));
+  }
   for (auto& b : ctx->host_free) free(b.first);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
