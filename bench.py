@@ -164,25 +164,57 @@ def committed_traffic(kernel, workload):
 
 
 def cpu_reference(A, B, target_products, steps, warmup):
-    """The reference's hybrid driver on rows [0, R): per-step GFLOP/s (its own phase timer)."""
+    """The reference's hybrid driver on rows [0, R): per-step GFLOP/s (its own phase timer).
+
+    Each run is the reference's four phases followed by freeing C, as its
+    driver does (src/ams_hybaccspgemm.c:316-343); C is never copied out."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle  # the reference built from its sources (oracle/_ref)
     R, P = sample_rows_for(A, B, target_products)
     As = slice_rows(A, 0, R)
+    timer = oracle.RefTimer(As, B, "hybacc", small=False)
     times = []
     for i in range(warmup + steps):
-        out = oracle.ref_spgemm(As, B, "hybacc", small=False)
-        if out is None:
+        rt = timer.run()
+        if rt is None:
             raise RuntimeError("sample below one morsel")
         if i >= warmup:
-            times.append(out[3]["total_time"])
-        del out
+            times.append(rt["total_time"])
     t = statistics.mean(times)
     info = oracle.ref_info("hybacc", small=False)
     return {"value": 2.0 * P / t / 1e9, "unit": "GFLOP/s", "cores": info["threads"], "kind": "reference",
             "sample": f"rows [0,{R}) of {A.num_row}: {P} products ({100.0 * P / max(1, total_products(A, B)):.1f}% "
                       f"of the workload), ams_hybaccspgemm kernels, {steps} runs after {warmup} warm-up, "
                       f"mean total_time {t:.3f} s"}
+
+
+def parity_blocks(A, B, gpu_rows, block_products):
+    """Row digests of the GPU product against the reference's own kernels on
+    three row blocks (start, middle, end) of about block_products products
+    each: the reference runs on A's rows of the block with B whole, its rows
+    are sorted and digested in the oracle (cas_csr_digest's row form)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    ps = row_products(A, B)
+    total = int(ps[-1])
+    m = A.num_row
+    blocks = []
+    for frac in (0.0, 0.5, 1.0):
+        start_p = min(max(0, int(total * frac) - (block_products if frac == 1.0 else 0)), total)
+        r0 = int(np.searchsorted(ps, start_p, side="left"))
+        r0 = min(r0, m - 1)
+        r1 = int(np.searchsorted(ps, int(ps[r0]) + block_products, side="left"))
+        r1 = max(r0 + 1, min(r1, m))
+        blocks.append((r0, r1))
+    out = {"blocks": [], "rows": 0, "match": True, "against": "reference ams_hybaccspgemm kernels (oracle/_ref), "
+                                                             "rows sorted, cas_csr_digest row digests"}
+    for r0, r1 in blocks:
+        res = oracle.ref_row_digests(slice_rows(A, r0, r1), B, "hybacc", small=True)
+        ok = res is not None and bool(np.array_equal(res[1], gpu_rows[r0:r1]))
+        out["blocks"].append({"rows": [r0, r1], "products": int(ps[r1] - ps[r0]), "match": ok})
+        out["rows"] += r1 - r0
+        out["match"] = out["match"] and ok
+    return out
 
 
 _TOTAL_P = {}
@@ -397,7 +429,9 @@ def main():
     ap.add_argument("--impl", default="cas", choices=["cas", "reference"])
     ap.add_argument("--workload", default="er_s21_ef32", choices=sorted(WORKLOADS))
     ap.add_argument("--accum", default="hybacc", choices=["hash", "hsersc", "hybacc"])
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--parity-products", type=float, default=3e7,
+                    help="products in each of the three row blocks checked against the reference")
     ap.add_argument("--ref-products", type=float, default=4e8,
                     help="products in the CPU reference's row sample")
     ap.add_argument("--row-fraction", type=float, default=1.0,
@@ -499,6 +533,11 @@ def main():
         P_total, nnz_total, launches_total = P_local, nnz_local, launches
     ms_step = elapsed_ms / args.steps
     value = 2.0 * P_total / (ms_step * 1e-3) / 1e9
+
+    # row digests of one product for the parity check against the reference
+    cc, _ = ctx.spgemm_device(dA, dB, args.accum)
+    _, gpu_rows = ctx.digest(cc, rows=True)
+    ctx.free(cc)
 
     # per-kernel times for the roofline: extra steps with the bins run one at
     # a time and each bin kernel timed by CUDA events on its stream
@@ -611,9 +650,14 @@ def main():
         dA = dB = None
         torch.cuda.empty_cache()
         try:
-            line["cpu_baseline"] = cpu_reference(A, B, args.ref_products, steps=1, warmup=1)
+            line["cpu_baseline"] = cpu_reference(A, B, args.ref_products, steps=3, warmup=1)
         except Exception as e:  # reported, not fatal
             line["cpu_baseline"] = {"value": None, "error": str(e)}
+        if args.row_fraction == 1.0:
+            try:
+                line["parity"] = parity_blocks(A, B, gpu_rows, int(args.parity_products))
+            except Exception as e:  # reported, not fatal
+                line["parity"] = {"match": None, "error": str(e)}
     ctx.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

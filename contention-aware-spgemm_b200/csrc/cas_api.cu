@@ -301,7 +301,18 @@ void* host_alloc_huge(size_t bytes) {
 // run at the DMA rate.
 constexpr double kHostCacheShare = 0.6;
 
+// Every cached block of every context is recorded in one process-wide map
+// from the block to the context that allocated it, and all host-block
+// bookkeeping (the map, and each context's host_blocks, host_free and
+// host_pinned) is changed under one mutex.  So a block can be returned through
+// any context, or none: cas_csr_free(NULL, C) or a call with another context
+// finds the owner, unregisters the block from CUDA if the owner had
+// registered it, and removes it from the owner's records before freeing it.
+std::mutex g_host_mu;
+std::unordered_map<void*, cas_ctx*> g_host_owner;
+
 void* host_take(cas_ctx* ctx, size_t bytes) {
+  std::lock_guard<std::mutex> lock(g_host_mu);
   size_t best = SIZE_MAX;
   size_t bi = 0;
   for (size_t i = 0; i < ctx->host_free.size(); ++i) {
@@ -318,7 +329,10 @@ void* host_take(cas_ctx* ctx, size_t bytes) {
     return p;
   }
   void* p = host_alloc_huge(bytes);
-  if (p) ctx->host_blocks[p] = bytes;
+  if (p) {
+    ctx->host_blocks[p] = bytes;
+    g_host_owner[p] = ctx;
+  }
   return p;
 }
 
@@ -362,17 +376,24 @@ void host_unpin(cas_ctx* ctx, void* p, size_t bytes) {
   }
 }
 
+// Returns a host block of a C.  A block of ctx's own cache goes back to it
+// (or is freed when the cache is full); a block of another context is
+// released from that context's records and freed; any other pointer is freed.
 void host_give(cas_ctx* ctx, void* p) {
   if (!p) return;
-  auto it = ctx ? ctx->host_blocks.find(p) : decltype(ctx->host_blocks)::iterator();
-  if (!ctx || it == ctx->host_blocks.end()) {
+  std::lock_guard<std::mutex> lock(g_host_mu);
+  auto own = g_host_owner.find(p);
+  if (own == g_host_owner.end()) {
     free(p);
     return;
   }
+  cas_ctx* owner = own->second;
+  auto it = owner->host_blocks.find(p);
   static const double phys = (double)sysconf(_SC_PHYS_PAGES) * (double)sysconf(_SC_PAGESIZE);
-  if ((double)(ctx->host_free_bytes + it->second) > kHostCacheShare * phys) {
-    host_unpin(ctx, p, it->second);
-    ctx->host_blocks.erase(it);
+  if (owner != ctx || (double)(owner->host_free_bytes + it->second) > kHostCacheShare * phys) {
+    host_unpin(owner, p, it->second);
+    owner->host_blocks.erase(it);
+    g_host_owner.erase(own);
     free(p);
     return;
   }
@@ -470,8 +491,13 @@ cas_status d2h_staged(cas_ctx* ctx, void* dst, const void* src, size_t bytes, bo
 
 // Device -> host copy of one output array: by DMA straight into a block the
 // context has registered, else through the staging buffers.
+bool host_is_pinned(cas_ctx* ctx, void* p) {
+  std::lock_guard<std::mutex> lock(g_host_mu);
+  return ctx->host_pinned.count(p) != 0;
+}
+
 cas_status d2h_out(cas_ctx* ctx, void* dst, const void* src, size_t bytes, bool widen = false) {
-  if (bytes > 0 && !widen && ctx->host_pinned.count(dst)) {
+  if (bytes > 0 && !widen && host_is_pinned(ctx, dst)) {
     CAS_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     ctx->d2h_direct += (double)bytes;
     return CAS_OK;
@@ -1203,12 +1229,17 @@ void cas_destroy(cas_ctx* ctx) {
     if (ctx->h_stage[i]) cudaFreeHost(ctx->h_stage[i]);
     if (ctx->ev_stage[i]) cudaEventDestroy(ctx->ev_stage[i]);
   }
-  // blocks still held by callers stay valid host memory, no longer registered
-  for (void* p : ctx->host_pinned) {
-    cudaHostUnregister(p);
-    g_pinned_bytes.fetch_sub(pin_length(ctx->host_blocks[p]));
+  {
+    // blocks still held by callers stay valid host memory, no longer
+    // registered and no longer recorded: cas_csr_free then just frees them
+    std::lock_guard<std::mutex> lock(g_host_mu);
+    for (void* p : ctx->host_pinned) {
+      cudaHostUnregister(p);
+      g_pinned_bytes.fetch_sub(pin_length(ctx->host_blocks[p]));
+    }
+    for (auto& b : ctx->host_blocks) g_host_owner.erase(b.first);
+    for (auto& b : ctx->host_free) free(b.first);
   }
-  for (auto& b : ctx->host_free) free(b.first);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
 }
@@ -1297,10 +1328,10 @@ cas_status cas_csr_free(cas_ctx* ctx, cas_csr* C) {
         cudaFree(C->rats);
       }
     } else {
-      cas_ctx* owner = C->owned == 2 ? ctx : nullptr;  // 2: blocks of this context's host cache
-      host_give(owner, C->row_ptrs);
-      host_give(owner, C->cols);
-      host_give(owner, C->rats);
+      // owned 2: blocks of a context's host cache; host_give finds their owner
+      host_give(ctx, C->row_ptrs);
+      host_give(ctx, C->cols);
+      host_give(ctx, C->rats);
     }
   }
   memset(C, 0, sizeof(*C));
@@ -1401,7 +1432,10 @@ cas_status cas_hybacc_numc(cas_ctx* ctx, const cas_csr* A, const cas_csr* B, con
 // process exits (kNoAllocParts partials, 128 KiB).  Every call overwrites the
 // partials it reads before reading them, so nothing needs clearing, and calls
 // that overlap on the GPU (on different streams, or from several host threads)
-// share the array and race: serialise them.
+// share the array and race: serialise them.  The array's device address is
+// looked up once per device and kept; after cudaDeviceReset (or any teardown
+// of the device's primary context) it is stale, so the function must not be
+// used again in that process.
 namespace {
 
 constexpr int64_t kNoAllocParts = 16384;  // scans of up to kNoAllocParts * kScanTile elements
@@ -1437,9 +1471,12 @@ extern "C" cas_status cas_scan_noalloc(int64_t* d_out, const int64_t* d_in, int6
     partial = g_noalloc_addr[dev];
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  cudaGetLastError();  // start from a clean error state, as the context entry points do
+  // an error the caller has not read yet stays theirs: report it, launch
+  // nothing, and leave it pending for the caller's own check
+  if (cudaPeekAtLastError() != cudaSuccess) return CAS_ERR_CUDA;
   cas::k_scan_partials<<<(unsigned)nparts, cas::kScanBlock, 0, s>>>(d_in, n - 1, partial);
   cas::k_scan_top<<<1, cas::kScanBlock, 0, s>>>(partial, nparts, nullptr);
   cas::k_scan_apply<<<(unsigned)nparts, cas::kScanBlock, 0, s>>>(d_in, n - 1, partial, d_out, n);
+  // a launch error here is this call's own: read it, and report it by status
   return cudaGetLastError() == cudaSuccess ? CAS_OK : CAS_ERR_CUDA;
 }

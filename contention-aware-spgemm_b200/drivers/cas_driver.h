@@ -22,8 +22,20 @@
  * with the same escape colours.  Fields the GPU adds come after the
  * reference's: gflops (2 * flop_cnt / total_time / 1e9), hbm_frac (the
  * Gustavson traffic model 12 nnz(A) + 12 flop + 12 nnz(C) + 16 (m + 1) bytes
- * over total_time, against CAS_PEAK_GBS), device.  As in the reference,
- * numc_perf and perf are flop_cnt per second of numc_time / total_time.
+ * over total_time, against the HBM peak), device, hbm_peak_gbs.  As in the
+ * reference, numc_perf and perf are flop_cnt per second of numc_time /
+ * total_time.
+ *
+ * The CONFIGURATION line carries the reference's fields first, in its order
+ * (HASH_CONSTANT .. HYB_THRES), so log parsers keyed on them keep working,
+ * then the GPU's (DRIVER, DEVICE, CUDA_DEVICE, SM_COUNT, RUN_NUM).  The
+ * reference's fields hold the values of the reference build whose output the
+ * driver reproduces, the per-driver settings of scripts/ams_rmat_run.sh:25-36
+ * with the build macros of scripts/ams_run_common.sh:20-33, except two that
+ * describe this run: THREAD_NUM is the GPU's resident thread count (SMs times
+ * threads per SM) and AMS_HIGH_THREAD_NUM the same share of it as the
+ * script's 16 or 22 of 64 threads; AMS_ACC_THRES is the value in use.  None
+ * of them changes the output: rows are sorted, and the sums are exact.
  *
  * The phases are timed on the device with CUDA events around the work the
  * reference times: A and B are loaded and resident before run 0, C is
@@ -34,8 +46,11 @@
  * and reuse a binary <dataset>.org.csr / .trs.csr beside the .mtx files), CAS_RUN_NUM (default 10,
  * at least 2, the reference's RUN_NUM), CAS_DEVICE (default 0),
  * CAS_VERIFY (1: VERIFYRESULT lines), CAS_ACC_THRES (hybrid threshold,
- * default 2.0 = the R-MAT scripts' value), CAS_PEAK_GBS (HBM bandwidth for
- * hbm_frac, default 6537.6, a copy kernel's rate measured on B200).
+ * default 2.0 = the R-MAT scripts' value), CAS_PEAK_GBS (HBM bandwidth in
+ * GB/s for hbm_frac); without it the driver reads "hbm_gbs" from the JSON
+ * file named by CAS_PEAKS_JSON (default ./MEASURED_PEAKS.json, a measured
+ * copy bandwidth), and failing that uses 6650, a copy kernel's rate measured
+ * on B200 earlier.
  * Failures print a message to stderr and exit with status 1, as the
  * reference's exit(1) does.
  */
@@ -149,16 +164,64 @@ static void drv_upload(const cas_csr *H, cas_csr *D) {
 	D->owned = 0;
 }
 
-static void drv_cfg_print(const char *driver, cas_accum acc, int device, const char *name, int sms, int run_num,
-                          double acc_thres) {
+/* The HBM bandwidth for hbm_frac: CAS_PEAK_GBS, else "hbm_gbs" of the JSON
+ * file CAS_PEAKS_JSON (default ./MEASURED_PEAKS.json), else 6650 GB/s. */
+static double drv_peak_gbs(void) {
+	const double env = drv_env_double("CAS_PEAK_GBS", 0.0);
+	if (env > 0) return env;
+	const char *path = getenv("CAS_PEAKS_JSON");
+	FILE *f = fopen((path && *path) ? path : "MEASURED_PEAKS.json", "r");
+	double v = 0.0;
+	if (f) {
+		char buf[8192];
+		const size_t n = fread(buf, 1, sizeof(buf) - 1, f);
+		fclose(f);
+		buf[n] = 0;
+		const char *k = strstr(buf, "\"hbm_gbs\"");
+		if (k && (k = strchr(k, ':'))) v = strtod(k + 1, NULL);
+	}
+	return v > 0 ? v : 6650.0;
+}
+
+/* Per-driver settings of the reference's R-MAT run script (scripts/ams_rmat_run.sh:25-36). */
+typedef struct {
+	int high_of_64;
+	double prt;
+	long smt_symb, smt_numc;
+} drv_script_cfg;
+
+static drv_script_cfg drv_script(cas_accum acc) {
+	if (acc == CAS_ACC_HASH) return (drv_script_cfg){16, 0.90, 11000000L, 2500000L};
+	return (drv_script_cfg){22, 0.85, 7000000L, 2100000L};
+}
+
+static void drv_cfg_print(const char *driver, cas_accum acc, int device, const struct cudaDeviceProp *prop,
+                          int run_num, double acc_thres) {
+	const drv_script_cfg sc = drv_script(acc);
+	const long threads = (long)prop->multiProcessorCount * prop->maxThreadsPerMultiProcessor;
 	printf("CONFIGURATION:");
-	printf("\tDRIVER: %s", driver);
-	printf("\tDEVICE: %s", name);
-	printf("\tCUDA_DEVICE: %d", device);
-	printf("\tSM_COUNT: %d", sms);
 	printf("\tHASH_CONSTANT: %ld", 2654435761L);
+	printf("\tTHREAD_NUM: %ld", threads);
+	printf("\tAMS_HIGH_THREAD_NUM: %ld", threads * sc.high_of_64 / 64);
+	printf("\tAMS_SIZE: %ld", 524288L);
+	printf("\tAMS_MIN_NUM: %ld", 32768L);
+	printf("\tAMS_PRT: %.6f", sc.prt);
+	printf("\tAMS_DNR");
+	printf("\tAMS_ACC_THRES: %.6f", acc == CAS_ACC_HYBACC ? acc_thres : 5.0);
+	printf("\tSMTACT");
+	printf("\tSMTACT_REAR");
+	printf("\tSMTACT_QUANTILE: %.6f", 0.99);
+	printf("\tSMTACT_SYMB_THRES: %ld", sc.smt_symb);
+	printf("\tSMTACT_NUMC_THRES: %ld", sc.smt_numc);
+	printf("\tDN_MIN: %ld", 256L);
+	printf("\tGUD_ALPHA: %.6f", 0.5);
+	printf("\tGUD_MIN: %ld", 256L);
+	printf("\tHYB_THRES: %.6f", 0.95);
+	printf("\tDRIVER: %s", driver);
+	printf("\tDEVICE: %s", prop->name);
+	printf("\tCUDA_DEVICE: %d", device);
+	printf("\tSM_COUNT: %d", prop->multiProcessorCount);
 	printf("\tRUN_NUM: %d", run_num);
-	if (acc == CAS_ACC_HYBACC) printf("\tAMS_ACC_THRES: %.6f", acc_thres);
 	printf("\n");
 }
 
@@ -174,7 +237,7 @@ static int cas_driver_main(int argc, char **argv, cas_accum acc, const char *dri
 	const int device = (int)drv_env_long("CAS_DEVICE", 0);
 	const int verify = (int)drv_env_long("CAS_VERIFY", 0);
 	const double acc_thres = drv_env_double("CAS_ACC_THRES", 2.0);
-	const double peak_gbs = drv_env_double("CAS_PEAK_GBS", 6537.6);
+	const double peak_gbs = drv_peak_gbs();
 	if (run_num < 2) drv_die("CAS_RUN_NUM must include a warm-up and at least one measured run");
 
 	char org[CAS_DRIVER_PATH_LEN], trs[CAS_DRIVER_PATH_LEN];
@@ -184,7 +247,7 @@ static int cas_driver_main(int argc, char **argv, cas_accum acc, const char *dri
 	struct cudaDeviceProp prop;
 	if (cudaSetDevice(device) != cudaSuccess || cudaGetDeviceProperties(&prop, device) != cudaSuccess)
 		drv_die("no usable CUDA device");
-	drv_cfg_print(driver, acc, device, prop.name, prop.multiProcessorCount, run_num, acc_thres);
+	drv_cfg_print(driver, acc, device, &prop, run_num, acc_thres);
 
 	cas_csr hA, hB, dA, dB;
 	drv_load(org, &hA);
@@ -252,10 +315,10 @@ static int cas_driver_main(int argc, char **argv, cas_accum acc, const char *dri
 	printf("dataset: %s\tnum_trials: %d\tthread_num: %d\tnuma_mask: %ld\t"
 	       "init_time: %.9f\tsymb_time: %.9f\tmgmt_time: %.9f\tnumc_time: %.9f\ttotal_time: %.9f\t"
 	       "flop_cnt: %ld\tnumc_perf: %.9f\tperf: %.9f\t"
-	       "gflops: %.3f\thbm_frac: %.4f\tdevice: %s\n",
+	       "gflops: %.3f\thbm_frac: %.4f\tdevice: %s\thbm_peak_gbs: %.1f\n",
 	       dataset, trials, prop.multiProcessorCount, 1L << device, sum.init_time / trials, sum.symb_time / trials,
 	       sum.mgmt_time / trials, numc, tot, (long)flop, flop / numc, flop / tot, 2.0 * flop / tot / 1e9,
-	       bytes / tot / (peak_gbs * 1e9), prop.name);
+	       bytes / tot / (peak_gbs * 1e9), prop.name, peak_gbs);
 	drv_reset();
 
 	cas_destroy(ctx);

@@ -167,14 +167,21 @@ cas_status cas_flp_populate(cas_ctx *ctx, const cas_csr *A, const cas_csr *B, in
  * Replaces scan (src/mm/mm_utils.c:903-957). */
 cas_status cas_scan(cas_ctx *ctx, int64_t *d_out, const int64_t *d_in, int64_t n);
 
-/* Exact distinct-column count of every row of A·B into d_row_nz (m entries),
- * given d_row_flp from cas_flp_populate.  Replaces ams_hash_symb_dnr
- * (src/ams/ams_utils.c:1701-1752) and ams_hash_symb (:483-602). */
+/* Exact distinct-column count of every row of A·B into d_row_nz (m entries).
+ * Replaces ams_hash_symb_dnr (src/ams/ams_utils.c:1701-1752) and
+ * ams_hash_symb (:483-602).  d_row_flp (from cas_flp_populate) is taken for
+ * the reference's signature and may be NULL: this call and the numeric calls
+ * below recompute the row products in the same pass that bins the rows by
+ * kernel, which reads A and B's row pointers once, so the caller's array is
+ * neither read nor written. */
 cas_status cas_hash_symb(cas_ctx *ctx, const cas_csr *A, const cas_csr *B, const int64_t *d_row_flp,
 	int64_t *d_row_nz);
 
 /* Numeric phase into a caller-allocated device C whose row_ptrs are the scan
- * of the symbolic counts (C->num_nnz entries of cols/rats).
+ * of the symbolic counts (C->num_nnz entries of cols/rats); d_row_flp as in
+ * cas_hash_symb.  Rows of more than 4096 distinct columns take the dense
+ * kernel, which builds its column bitmaps itself here (cas_spgemm keeps them
+ * from its symbolic pass).
  * Replace ams_hash_numc (src/ams/ams_utils.c:608-774), ams_hsersc_numc
  * (:781-949) and ams_hybacc_numc (:1159-1338). */
 cas_status cas_hash_numc(cas_ctx *ctx, const cas_csr *A, const cas_csr *B, const int64_t *d_row_flp,
@@ -202,7 +209,9 @@ cas_status cas_spgemm(cas_ctx *ctx, cas_accum accum, const cas_csr *A, const cas
  * made them, which keeps up to 60% of physical memory of such blocks, pages
  * resident, for later outputs (so repeated products into host memory skip
  * the page faults); they are released at cas_destroy.  Passing another
- * context or NULL frees them at once. */
+ * context or NULL frees them at once, after releasing them from the context
+ * that made them (and unregistering them from CUDA where it had registered
+ * them); this is safe from any thread. */
 cas_status cas_csr_free(cas_ctx *ctx, cas_csr *C);
 
 /* ---- digests of a product ------------------------------------------------
@@ -339,6 +348,13 @@ void cas_serve_destroy(cas_server *srv);
  *     the default stream); synchronise before reading d_out.
  *   - All calls share the one array: calls that may overlap on the GPU must
  *     be serialised by the caller.
+ *   - The array's address is looked up once per device and kept, so the
+ *     function must not be used after cudaDeviceReset (or any other teardown
+ *     of the device's primary context) in the same process.
+ *   - A CUDA error already pending on the calling thread makes the call
+ *     return CAS_ERR_CUDA without launching, and stays pending for the
+ *     caller; an error of the call's own launches is read (cleared) and
+ *     reported as CAS_ERR_CUDA.
  * No counterpart in the reference: its scan (src/mm/mm_utils.c:903) runs on
  * the host and allocates nothing on a device to begin with. */
 cas_status cas_scan_noalloc(int64_t *d_out, const int64_t *d_in, int64_t n, void *stream);

@@ -418,3 +418,31 @@ void orc_free(orc_csr *C) {
 	free(C->rats);
 	memset(C, 0, sizeof(orc_csr));
 }
+
+/* SplitMix64 finaliser (Steele, Lea, Flood 2014), as the casgemm digests use it. */
+static uint64_t orc_mix64(uint64_t z) {
+	z += 0x9E3779B97F4A7C15ull;
+	z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+	z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+	return z ^ (z >> 31);
+}
+
+uint64_t orc_row_digests(const orc_csr *C, int64_t row_offset, uint64_t *row_digests) {
+	uint64_t total = 0;
+	#pragma omp parallel for schedule(dynamic, 1024) reduction(+ : total)
+	for (int64_t i = 0; i < C->num_row; i++) {
+		int64_t s = C->row_ptrs[i], e = C->row_ptrs[i + 1];
+		uint64_t h = 0;
+		for (int64_t j = s; j < e; j++) {
+			uint64_t bits;
+			memcpy(&bits, &C->rats[j], sizeof(bits));
+			h += orc_mix64((uint64_t) C->cols[j] * 0x9E3779B97F4A7C15ull + (uint64_t) (j - s)) ^
+				orc_mix64(bits + 0x632BE59BD9B4E019ull);
+		}
+		if (row_digests) {
+			row_digests[i] = h;
+		}
+		total += orc_mix64(h + (uint64_t) (i + row_offset));
+	}
+	return total;
+}

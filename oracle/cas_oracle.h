@@ -82,6 +82,17 @@ int64_t orc_pack_morsels(int64_t num_row, const int64_t *ps_weight, const int64_
 	const int64_t *ps_flp, int64_t morsel, double prt, int64_t *bounds, double *cf,
 	int64_t *maxflp, int64_t *order, int64_t *low_head, int64_t *high_tail);
 
+/* Row digests of C in the form of the casgemm ABI's cas_csr_digest (no
+ * counterpart in the reference, whose IN_VERIFY build prints only nnz, the
+ * column sum and the value sum, src/ams_hashspgemm.c:307-318):
+ *   h(c, k, v) = mix64(c * 0x9E3779B97F4A7C15 + k) ^ mix64(bits(v) + 0x632BE59BD9B4E019)
+ *   row_digests[r] = sum over the row's entries in stored order, k = 0, 1, ...
+ * with mix64 the SplitMix64 finaliser (Steele, Lea, Flood 2014), bits(v) the
+ * fp64 bit pattern, sums modulo 2^64.  Rows should be sorted first
+ * (orc_sort_rows) for a canonical digest.  Returns the product digest
+ * sum over r of mix64(row_digests[r] + r + row_offset). */
+uint64_t orc_row_digests(const orc_csr *C, int64_t row_offset, uint64_t *row_digests);
+
 void orc_free(orc_csr *C);
 
 #ifdef __cplusplus

@@ -63,6 +63,8 @@ def _load_oracle():
         lib.orc_next_pow2.restype = ctypes.c_int64
         lib.orc_next_pow2.argtypes = [ctypes.c_int64]
         lib.orc_radix_sort_kv.argtypes = [P, P, P, P, ctypes.c_int64]
+        lib.orc_row_digests.restype = ctypes.c_uint64
+        lib.orc_row_digests.argtypes = [ctypes.POINTER(OrcCsr), ctypes.c_int64, P]
         lib.orc_pack_morsels.restype = ctypes.c_int64
         lib.orc_pack_morsels.argtypes = [ctypes.c_int64, P, P, P, ctypes.c_int64, ctypes.c_double, P, P, P, P,
                                          ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
@@ -153,12 +155,67 @@ def ref_spgemm(A, B, algo: str = "hybacc", small: bool = True):
     if st != 0:
         return None
     try:
+        _load_oracle().orc_sort_rows(ctypes.byref(c))  # csr_t and orc_csr share one layout
         rp, cols, vals = _from_orc(c)
     finally:
         lib.ref_free_csr(ctypes.byref(c))
     del ka, kb
-    rp, cols, vals = sort_rows(rp, cols, vals)
     return rp, cols, vals, {n: getattr(rt, n) for n, _ in RefRuntime._fields_}
+
+
+class RefTimer:
+    """Times the reference's own driver sequence on fixed inputs, the way its
+    drivers do: each run builds C and frees it again
+    (src/ams_hybaccspgemm.c:316-343), and only the reference's runtime_t is
+    kept.  The csr_t views of A and B are built once, so a run costs the
+    reference's four phases plus its own free_csr, with no copy of C into
+    Python and no per-row sort."""
+
+    def __init__(self, A, B, algo: str = "hybacc", small: bool = False):
+        self.lib = _load_ref(algo, small)
+        self.a, self.ka = to_orc(A.row_ptrs, A.cols, A.vals, A.num_col)
+        self.b, self.kb = to_orc(B.row_ptrs, B.cols, B.vals, B.num_col)
+
+    def run(self) -> Optional[dict]:
+        """One run; the runtime dict, or None when A is below one morsel."""
+        c = OrcCsr()
+        rt = RefRuntime()
+        st = self.lib.ref_spgemm(ctypes.byref(self.a), ctypes.byref(self.b), ctypes.byref(c), ctypes.byref(rt))
+        if st != 0:
+            return None
+        nnz = int(c.num_nnz)
+        self.lib.ref_free_csr(ctypes.byref(c))
+        out = {n: getattr(rt, n) for n, _ in RefRuntime._fields_}
+        out["nnz_c"] = nnz
+        return out
+
+
+def ref_row_digests(A, B, algo: str = "hybacc", small: bool = False, row_offset: int = 0):
+    """C = A*B by the reference's own kernels, reduced to the row digests of
+    the casgemm ABI (cas_csr_digest) after sorting each row by column, in C
+    with OpenMP, so that outputs of hundreds of millions of entries are
+    checked without copying them into Python.
+
+    Returns (row_ptrs, row digests uint64[m], digest, runtime dict) or None
+    below one morsel; `digest` counts row r as r + row_offset."""
+    lib = _load_ref(algo, small)
+    orc = _load_oracle()
+    a, ka = to_orc(A.row_ptrs, A.cols, A.vals, A.num_col)
+    b, kb = to_orc(B.row_ptrs, B.cols, B.vals, B.num_col)
+    c = OrcCsr()
+    rt = RefRuntime()
+    st = lib.ref_spgemm(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(rt))
+    if st != 0:
+        return None
+    try:
+        orc.orc_sort_rows(ctypes.byref(c))
+        rp = np.ctypeslib.as_array(ctypes.cast(c.row_ptrs, ctypes.POINTER(ctypes.c_int64)), (c.num_row + 1,)).copy()
+        rows = np.zeros(c.num_row, np.uint64)
+        total = int(orc.orc_row_digests(ctypes.byref(c), int(row_offset), rows.ctypes.data))
+    finally:
+        lib.ref_free_csr(ctypes.byref(c))
+    del ka, kb
+    return rp, rows, total, {n: getattr(rt, n) for n, _ in RefRuntime._fields_}
 
 
 def ref_load_mtx(path: str):

@@ -103,6 +103,10 @@ def test_driver_matches_reference_log(tmp_path, algo):
     assert p.returncode == 0, p.stderr
     ref = open(os.path.join(GOLDEN, f"driver_{algo}_g500_12_8.log")).read()
     assert p.stdout.startswith("CONFIGURATION:")
+    # the reference's configuration keys, in its order, ahead of the GPU's
+    cfg_keys = lambda text: [f.split(": ")[0] for f in text.splitlines()[0].split("\t")[1:]]  # noqa: E731
+    assert cfg_keys(p.stdout)[:len(cfg_keys(ref))] == cfg_keys(ref)
+    assert cfg_keys(p.stdout)[len(cfg_keys(ref)):] == ["DRIVER", "DEVICE", "CUDA_DEVICE", "SM_COUNT", "RUN_NUM"]
     runs = [RUN_LINE.match(x) for x in p.stdout.splitlines() if "th run" in x]
     assert len(runs) == 3 and all(runs)
     assert [int(m.group(1)) for m in runs] == [0, 1, 2]
@@ -115,7 +119,7 @@ def test_driver_matches_reference_log(tmp_path, algo):
     assert [k for k, _ in ours[:len(theirs)]] == [k for k, _ in theirs]
     assert dict(ours)["flop_cnt"] == dict(theirs)["flop_cnt"]
     assert dict(ours)["dataset"] == "g500_12_8" and dict(ours)["num_trials"] == "2"
-    assert [k for k, _ in ours[len(theirs):]] == ["gflops", "hbm_frac", "device"]
+    assert [k for k, _ in ours[len(theirs):]] == ["gflops", "hbm_frac", "device", "hbm_peak_gbs"]
     # the binary cache written by this run serves the next one with the same result
     assert (ds / "g500_12_8.org.csr").exists() and (ds / "g500_12_8.trs.csr").exists()
     q = subprocess.run([os.path.join(BIN, ALGOS[algo]), "g500_12_8"], cwd=tmp_path, capture_output=True, text=True,

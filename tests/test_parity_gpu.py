@@ -90,3 +90,59 @@ def test_host_output_dma_into_kept_blocks(ctx):
     third = ctx.spgemm(A, B, "hybacc", col_bytes=8)
     np.testing.assert_array_equal(third.csr.cols, ref[1])
     np.testing.assert_array_equal(third.csr.vals, ref[2])
+
+
+def _raw_host_product(ctx, ca, cb):
+    """cas_spgemm into host memory through the C ABI; the caller frees C."""
+    import ctypes
+    cc = casgemm.CasCsr()
+    cc.on_device, cc.col_bytes = 0, 4
+    st = ctx.lib.cas_spgemm(ctx.h, casgemm.ACCUM["hybacc"], ctypes.byref(ca), ctypes.byref(cb), ctypes.byref(cc),
+                            None)
+    assert st == 0, ctx.lib.cas_last_error(ctx.h).decode()
+    return cc
+
+
+def _host_arrays(cc):
+    import ctypes
+    m, nnz = cc.num_row, cc.num_nnz
+    rp = np.ctypeslib.as_array(ctypes.cast(cc.row_ptrs, ctypes.POINTER(ctypes.c_int64)), (m + 1,)).copy()
+    cols = np.ctypeslib.as_array(ctypes.cast(cc.cols, ctypes.POINTER(ctypes.c_int32)), (nnz,)).astype(np.int64)
+    vals = np.ctypeslib.as_array(ctypes.cast(cc.rats, ctypes.POINTER(ctypes.c_double)), (nnz,)).copy()
+    return rp, cols, vals
+
+
+def test_registered_block_freed_without_its_context():
+    """A C whose host blocks the context has registered with CUDA may be freed
+    with no context (cas_csr_free(NULL, C)): the blocks are unregistered and
+    dropped from the producing context's cache first, so its next output goes
+    to fresh blocks (no direct DMA) and is still exact; after a free through
+    the context, outputs land in registered blocks again."""
+    import ctypes
+    from conftest import has_gpu
+    if not has_gpu():
+        pytest.skip("no CUDA device")
+    ctx = casgemm.Context(0)  # a context of its own: its block cache starts empty
+    A = casgemm.gen_er(14, 32, 9)
+    B = A.transpose()
+    ref = oracle.oracle_spgemm(A, B, "hybacc")
+    ca, cb = A.as_cas(), B.as_cas()
+    c1 = _raw_host_product(ctx, ca, cb)
+    ctx.lib.cas_csr_free(ctx.h, ctypes.byref(c1))           # into the cache, registered
+    c2 = _raw_host_product(ctx, ca, cb)                      # lands in the registered blocks
+    assert ctx.stats()["d2h_direct_bytes"] >= 8 * c2.num_nnz
+    got = _host_arrays(c2)
+    assert ctx.lib.cas_csr_free(None, ctypes.byref(c2)) == 0  # no context: released from ctx's records
+    for x, y in zip(got, ref[:3]):
+        np.testing.assert_array_equal(x, y)
+    c3 = _raw_host_product(ctx, ca, cb)
+    assert ctx.stats()["d2h_direct_bytes"] == 0              # fresh blocks, nothing registered
+    for x, y in zip(_host_arrays(c3), ref[:3]):
+        np.testing.assert_array_equal(x, y)
+    ctx.lib.cas_csr_free(ctx.h, ctypes.byref(c3))
+    c4 = _raw_host_product(ctx, ca, cb)
+    assert ctx.stats()["d2h_direct_bytes"] >= 8 * c4.num_nnz
+    for x, y in zip(_host_arrays(c4), ref[:3]):
+        np.testing.assert_array_equal(x, y)
+    ctx.lib.cas_csr_free(ctx.h, ctypes.byref(c4))
+    ctx.close()

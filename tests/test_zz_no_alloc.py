@@ -66,3 +66,26 @@ def test_noalloc_scan_rejects_oversize(ctx):
     # rejected before any memory is touched, so the small arrays are safe here
     st = _noalloc(ctx.lib)(small.data_ptr(), small.data_ptr(), MAX_N + 1, None)
     assert st == CAS_ERR_REJECTED
+
+
+def test_noalloc_scan_at_the_size_limit(ctx):
+    """n == MAX_N: the last of the 16,384 tile sums fills the array's last slot."""
+    import torch
+
+    n = MAX_N
+    g = torch.Generator(device="cuda").manual_seed(7)
+    d_in = torch.randint(0, 4, (n - 1,), dtype=torch.int64, device="cuda", generator=g)
+    out = torch.full((n,), -1, dtype=torch.int64, device="cuda")
+    ref = torch.full((n,), -2, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):  # twice in a row through the shared scratch
+        out.fill_(-1)
+        assert _noalloc(ctx.lib)(out.data_ptr(), d_in.data_ptr(), n, stream) == 0
+        torch.cuda.synchronize()
+        assert ctx.lib.cas_scan(ctx.h, ref.data_ptr(), d_in.data_ptr(), n) == 0
+        torch.cuda.synchronize()
+        assert torch.equal(out, ref)
+    assert int(out[0]) == 0
+    assert int(out[-1]) == int(d_in.sum())
+    assert int(out[n // 2]) == int(d_in[: n // 2].sum())
+
