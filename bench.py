@@ -438,6 +438,8 @@ def main():
                     help="use only the first fraction of A's rows (profiling captures; B stays whole)")
     ap.add_argument("--tune", default=None, metavar="CACHE.json",
                     help="pick the row routing with casgemm.Autotuner (cached in CACHE.json) before timing")
+    ap.add_argument("--esc-form", type=int, default=None, choices=[0, 1, 2],
+                    help="bucketed ESC kernel form (cas_tuning.esc_form); default: the library's")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -484,6 +486,8 @@ def main():
     ctx.set_stream(stream.cuda_stream)
 
     tuning = None
+    if args.esc_form is not None:
+        ctx.set_tuning(esc_form=args.esc_form)
     if args.tune:
         tuner = casgemm.Autotuner(ctx, args.tune)
         key = casgemm.Autotuner.key(As, B)
@@ -566,14 +570,18 @@ def main():
     kernel_name = {"tiny": "k_numc_tiny<256>", "hash256": "k_numc_hash<256,9>", "hash1k": "k_numc_hash<256,11>",
                    "hash4k": "k_numc_hash<512,13>", "dense": "k_numc_dense<512>"}.get(dom)
     # the index form runs the fused rows and the ESC bins over 4096 products when esc_form is 1
-    idx_form = ctx.get_tuning().get("esc_form", 1) == 1
+    form = ctx.get_tuning().get("esc_form", 1)
+    idx_form = form >= 1
     if dom == "fused":
-        kernel_name = "k_numc_esc_%s<256,4800,11,fused>" % ("idx" if idx_form else "msd")
+        kernel_name = "k_numc_esc_%s<256,4800,11,fused%s>" % ("idx" if idx_form else "msd",
+                                                            ",keys in registers" if form == 2 else "")
     if kernel_name is None and dom.startswith("esc"):
         shape = {"esc1k": "1024,9", "esc2k": "2048,9", "esc3k": "3072,10", "esc4k": "4096,10",
                  "esc5k": "4800,11", "esc6k": "6144,11", "esc8k": "8192,11"}[dom]
         big = dom in ("esc5k", "esc6k", "esc8k")
-        kernel_name = "k_numc_esc_%s<256,%s>" % ("idx" if idx_form and big else "msd", shape)
+        kernel_name = "k_numc_esc_%s<256,%s%s>" % ("idx" if idx_form and big else "msd", shape,
+                                                  ",keys in registers" if form == 2 and dom in ("esc5k", "esc6k")
+                                                  else "")
     alg_bytes_total = 12.0 * (A.nnz if world == 1 else As.nnz) + 12.0 * P_local + 12.0 * nnz_local + 16.0 * (As.num_row + 1)
     pipe_frac = alg_bytes_total / (ms_step * 1e-3) / (peak * 1e9)
 

@@ -70,7 +70,8 @@ struct cas_ctx {
   bool fuse = true;                        // fused ESC rows (no symbolic pass) in cas_spgemm
   int fused_lo = (int)cas::kFusedLo;       // fused rows: more products than this (up to kFusedHi)
   int esc_form = 1;                        // bucketed ESC of rows over 4096 products (fused rows included):
-                                           // 1 index form (k_numc_esc_idx), 0 k_numc_esc_msd
+                                           // 1 index form (k_numc_esc_idx), 0 k_numc_esc_msd, 2 the index
+                                           // form with the keys in registers between its two key passes
   int esc_max = 8192;                      // ESC rows: at most this many products
   int hash_max = 4096;                     // hash rows: at most this many distinct columns
   double acc_thres = 2.0;
@@ -223,12 +224,16 @@ cas_status setup_numc_kernels(cas_ctx* ctx) {
   using namespace cas;
 #define CAS_SETUP_ESC(bin, CAP, NBB)                                                               \
   CAS_TRY(allow_smem(ctx, k_numc_esc_msd<256, CAP, NBB, VIn>, smem_numc_esc_msd<CAP, NBB, VIn>())); \
-  if constexpr (CAP > 4096) CAS_TRY(allow_smem(ctx, k_numc_esc_idx<256, CAP, NBB, VIn>, smem_numc_esc_idx<CAP, NBB, VIn>()));
+  if constexpr (CAP > 4096) CAS_TRY(allow_smem(ctx, k_numc_esc_idx<256, CAP, NBB, VIn>, smem_numc_esc_idx<CAP, NBB, VIn>())); \
+  if constexpr (CAP > 4096 && CAP <= 6144)                                                         \
+    CAS_TRY(allow_smem(ctx, k_numc_esc_idx<256, CAP, NBB, VIn, false, true>, smem_numc_esc_idx<CAP, NBB, VIn>()));
   CAS_ESC_SHAPES(CAS_SETUP_ESC)
 #undef CAS_SETUP_ESC
   CAS_TRY(allow_smem(ctx, k_numc_esc_msd<256, (int)kFusedHi, 11, VIn, true>,
                      smem_numc_esc_msd<(int)kFusedHi, 11, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_esc_idx<256, (int)kFusedHi, 11, VIn, true>,
+                     smem_numc_esc_idx<(int)kFusedHi, 11, VIn>()));
+  CAS_TRY(allow_smem(ctx, k_numc_esc_idx<256, (int)kFusedHi, 11, VIn, true, true>,
                      smem_numc_esc_idx<(int)kFusedHi, 11, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_esc_overflow<1024, 8192, VIn>, smem_numc_esc<1024, 8192, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_hash<256, 9, VIn>, smem_numc_hash<256, 9, VIn>()));
@@ -761,6 +766,11 @@ cas_status launch_fused(cas_ctx* ctx, Call& c, const int64_t* known, int32_t* cc
         <<<(unsigned)c.nf, 256, smem_numc_esc_idx<(int)kFusedHi, 11, VIn>(), ctx->stream>>>(
             nullptr, c.A.csr, c.B.csr, c.b_sorted ? 1 : 0, nullptr, ccol, static_cast<AT*>(cval), c.ovf, ovf_count,
             ctx->d_status, fu);
+  else if (ctx->esc_form == 2)
+    k_numc_esc_idx<256, (int)kFusedHi, 11, VIn, true, true>
+        <<<(unsigned)c.nf, 256, smem_numc_esc_idx<(int)kFusedHi, 11, VIn>(), ctx->stream>>>(
+            nullptr, c.A.csr, c.B.csr, c.b_sorted ? 1 : 0, nullptr, ccol, static_cast<AT*>(cval), c.ovf, ovf_count,
+            ctx->d_status, fu);
   else
     k_numc_esc_msd<256, (int)kFusedHi, 11, VIn, true>
         <<<(unsigned)c.nf, 256, smem_numc_esc_msd<(int)kFusedHi, 11, VIn>(), ctx->stream>>>(
@@ -877,8 +887,15 @@ void launch_esc_bin(int esc_form, int64_t n, cudaStream_t s, const int32_t* rows
                     int32_t b_sorted, const int64_t* crp, int32_t* ccol, typename cas::Acc<VIn>::T* cval, int32_t* ovf,
                     unsigned int* ovf_count, cas::DevStatus* st) {
   using namespace cas;
+  if constexpr (CAP > 4096 && CAP <= 6144) {
+    if (esc_form == 2) {
+      k_numc_esc_idx<256, CAP, NBB, VIn, false, true><<<(unsigned)n, 256, smem_numc_esc_idx<CAP, NBB, VIn>(), s>>>(
+          rows, A, B, b_sorted, crp, ccol, cval, ovf, ovf_count, st, Fused{});
+      return;
+    }
+  }
   if constexpr (CAP > 4096) {
-    if (esc_form == 1) {
+    if (esc_form >= 1) {
       k_numc_esc_idx<256, CAP, NBB, VIn><<<(unsigned)n, 256, smem_numc_esc_idx<CAP, NBB, VIn>(), s>>>(
           rows, A, B, b_sorted, crp, ccol, cval, ovf, ovf_count, st, Fused{});
       return;
@@ -1262,7 +1279,7 @@ cas_status cas_set_tuning(cas_ctx* ctx, const cas_tuning* t) {
   if (!ctx || !t) return CAS_ERR_BAD_INPUT;
   if (!(t->acc_thres >= 0.0) || t->fused_min_products < 32 || t->fused_min_products >= (int)cas::kFusedHi ||
       t->esc_max_products < 32 || t->esc_max_products > 8192 || t->hash_max_nnz < 0 || t->hash_max_nnz > 4096 ||
-      (t->esc_form != 0 && t->esc_form != 1))
+      t->esc_form < 0 || t->esc_form > 2)
     return set_err(ctx, CAS_ERR_BAD_INPUT, "tuning out of range");
   ctx->acc_thres = t->acc_thres;
   ctx->fuse = t->fusion != 0;

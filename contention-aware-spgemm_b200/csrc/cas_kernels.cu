@@ -1406,6 +1406,39 @@ __device__ __forceinline__ void expand_values(const Csr& B, int total, const Sta
   }
 }
 
+// The same values, a warp per B row (segment) of the staged chunk: the
+// segment's start, first product and A value are read once per warp, and
+// the lanes load the row's values with consecutive addresses.  Two segments
+// are in flight per warp.  Suits chunks whose B rows are long (the lanes of a
+// short row idle); f(a, b, p) as in expand_values.
+template <int BLOCK, typename VIn, typename F>
+__device__ __forceinline__ void expand_values_seg(const Csr& B, int na, const StageB<VIn>& sg, F&& f) {
+  constexpr int NW = BLOCK / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const VIn* __restrict__ bval = static_cast<const VIn*>(B.val);
+  for (int s0 = warp; s0 < na; s0 += 2 * NW) {
+    const int s1 = s0 + NW;
+    const int b0 = sg.pre[s0], l0 = sg.pre[s0 + 1] - b0;
+    const int b1 = s1 < na ? sg.pre[s1] : 0, l1 = s1 < na ? sg.pre[s1 + 1] - b1 : 0;
+    const VIn a0 = sg.av[s0], a1 = s1 < na ? sg.av[s1] : VIn(0);
+    const VIn* __restrict__ r0 = bval + sg.bs[s0];
+    const VIn* __restrict__ r1 = bval + (s1 < na ? sg.bs[s1] : 0);
+    const int lmax = l0 > l1 ? l0 : l1;
+    for (int i = lane; i < lmax; i += 64) {
+      const int j = i + 32;
+      VIn v[4];
+      v[0] = i < l0 ? __ldg(r0 + i) : VIn(0);
+      v[1] = j < l0 ? __ldg(r0 + j) : VIn(0);
+      v[2] = i < l1 ? __ldg(r1 + i) : VIn(0);
+      v[3] = j < l1 ? __ldg(r1 + j) : VIn(0);
+      if (i < l0) f(a0, v[0], b0 + i);
+      if (j < l0) f(a0, v[1], b0 + j);
+      if (i < l1) f(a1, v[2], b1 + i);
+      if (j < l1) f(a1, v[3], b1 + j);
+    }
+  }
+}
+
 template <int N>
 __device__ __forceinline__ void sort_perm_small(uint32_t* __restrict__ skey, uint16_t* __restrict__ sidx, int s, int e,
                                                 uint32_t kbase) {
@@ -1459,7 +1492,7 @@ __device__ __forceinline__ void warp_sort_perm(uint32_t* __restrict__ skey, uint
   __syncwarp();
 }
 
-template <int BLOCK, int CAP, int NBB, typename VIn, bool FUSED = false>
+template <int BLOCK, int CAP, int NBB, typename VIn, bool FUSED = false, bool REGK = false>
 __global__ void __launch_bounds__(BLOCK, kIdxMinBlocks)
 k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted, const int64_t* __restrict__ crp,
                int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval,
@@ -1575,11 +1608,29 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   const uint32_t lo = sg.kmin;
   const int bits = (sg.kmax > sg.kmin) ? 32 - __clz(sg.kmax - sg.kmin) : 0;
   const int shift = bits > NBB ? bits - NBB : 0;
-  // pass 1: keys only, bucket histogram
+  // pass 1: keys only, bucket histogram.  REGK: the thread's keys (products
+  // threadIdx.x + u * BLOCK) stay in registers for pass 2, so B's columns
+  // are read once
   int huge;
-  expand_chunk<BLOCK, false, VIn>(B, n, sg, segof, [&](int32_t key, VIn, VIn, int) {
-    bucket_add(bcnt, (int)(((uint32_t)key - lo) >> shift));
-  });
+  constexpr int NPT = REGK ? (CAP + BLOCK - 1) / BLOCK : 1;
+  uint32_t rkey[NPT];
+  if constexpr (REGK) {
+#pragma unroll
+    for (int u = 0; u < NPT; ++u) {
+      const int p = threadIdx.x + u * BLOCK;
+      if (p < n) {
+        const int sgi = segof[p];
+        rkey[u] = (uint32_t)__ldg(B.col + sg.bs[sgi] + (p - sg.pre[sgi]));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < NPT; ++u)
+      if (threadIdx.x + u * BLOCK < n) bucket_add(bcnt, (int)((rkey[u] - lo) >> shift));
+  } else {
+    expand_chunk<BLOCK, false, VIn>(B, n, sg, segof, [&](int32_t key, VIn, VIn, int) {
+      bucket_add(bcnt, (int)(((uint32_t)key - lo) >> shift));
+    });
+  }
   __syncthreads();
   // exclusive scan of the bucket counts: NB / BLOCK consecutive buckets per thread
   constexpr int WPT = NB / (2 * BLOCK);
@@ -1611,11 +1662,23 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   }
   __syncthreads();
   // pass 2: (column, product index) into bucket order
-  expand_chunk<BLOCK, false, VIn>(B, n, sg, segof, [&](int32_t key, VIn, VIn, int p) {
-    const int pos = (int)bucket_add(bcnt, (int)(((uint32_t)key - lo) >> shift));
-    skey[pos] = (uint32_t)key;
-    sidx[pos] = (uint16_t)p;
-  });
+  if constexpr (REGK) {
+#pragma unroll
+    for (int u = 0; u < NPT; ++u) {
+      const int p = threadIdx.x + u * BLOCK;
+      if (p < n) {
+        const int pos = (int)bucket_add(bcnt, (int)((rkey[u] - lo) >> shift));
+        skey[pos] = rkey[u];
+        sidx[pos] = (uint16_t)p;
+      }
+    }
+  } else {
+    expand_chunk<BLOCK, false, VIn>(B, n, sg, segof, [&](int32_t key, VIn, VIn, int p) {
+      const int pos = (int)bucket_add(bcnt, (int)(((uint32_t)key - lo) >> shift));
+      skey[pos] = (uint32_t)key;
+      sidx[pos] = (uint16_t)p;
+    });
+  }
   __syncthreads();
   // sort each bucket: a lane per bucket of 2..8 pairs (one network size per
   // warp), then the warp's buckets of 9..kBucketLimit pairs one at a time;
@@ -1758,14 +1821,17 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
     }
   }
   __syncthreads();
-  // product order: a_ik * b_kj to its place
-  expand_values<BLOCK, VIn>(B, n, sg, segof, [&](VIn av, VIn bv, int p) {
+  // product order: a_ik * b_kj to its place (REGK: a warp per B row when
+  // the chunk's B rows average at least 32 products)
+  auto put = [&](VIn av, VIn bv, int p) {
     const uint16_t o = place_of[p];
     if (o == kSkip) return;
     const AT v = Acc<VIn>::mul(av, bv);
     if (o & kShared) Acc<VIn>::atomic_add(&cval[c0 + (o & ~kShared)], v);
     else cval[c0 + o] = v;
-  });
+  };
+  if (REGK && n >= 32 * (int)(ae - as)) expand_values_seg<BLOCK, VIn>(B, (int)(ae - as), sg, put);
+  else expand_values<BLOCK, VIn>(B, n, sg, segof, put);
   if (!FUSED && threadIdx.x == 0 && distinct != nz)
     dev_report(st, distinct > nz ? kDevRowOverflow : kDevRowUnderflow, 16, r);
 }

@@ -249,3 +249,35 @@ def test_index_form_many_shared_columns(ctx, per_b):
             same(out, ref)
     finally:
         ctx.set_tuning(**saved)
+
+
+def _register_form_cases():
+    er = casgemm.gen_er(13, 32, 7)
+    er_wide = casgemm.gen_er(12, 40, 3)   # rows of 4801..6144 products: the 6144 bin
+    g500 = casgemm.gen_g500(12, 16, 5)   # short B rows: the product-order value pass
+    hotA, hotB = hot_column_matrix(per_row=120, hot=2)
+    return [("er_s13_ef32", er, er.transpose()), ("er_s12_ef40", er_wide, er_wide.transpose()),
+            ("g500_s12_ef16", g500, g500.transpose()), ("hot_columns", hotA, hotB),
+            ("g500_int", with_int_values(g500, 9), with_int_values(g500, 9).transpose())]
+
+
+@pytest.mark.parametrize("fuse", [True, False])
+@pytest.mark.parametrize("case", range(5), ids=["er_s13_ef32", "er_s12_ef40", "g500_s12_ef16", "hot_columns",
+                                                  "g500_int"])
+def test_register_form_matches_oracle(ctx, case, fuse):
+    """esc_form 2: the index form with each thread's keys held in registers
+    between the histogram and the scatter, and (for long B rows) a warp per B
+    row in the value pass; fused rows and the 4800 / 6144 ESC bins."""
+    name, A, B = _register_form_cases()[case]
+    ref = oracle.oracle_spgemm(A, B, "hybacc")
+    saved = ctx.get_tuning()
+    ctx.set_tuning(fusion=int(fuse), esc_form=2)
+    try:
+        out = ctx.spgemm(A, B, "hybacc")
+        again = ctx.spgemm(A, B, "hsersc")
+    finally:
+        ctx.set_tuning(**saved)
+    same(out, ref)
+    same(again, oracle.oracle_spgemm(A, B, "hsersc"))
+    if fuse and name.startswith("er_s13"):
+        assert out.stats["fused_rows"] > A.num_row // 2

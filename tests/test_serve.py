@@ -137,13 +137,17 @@ def test_chunked_request_equals_alone():
 def test_small_requests_pass_a_large_one():
     if not has_gpu():
         pytest.skip("no CUDA device")
-    big = casgemm.gen_g500(16, 16, 3)
+    # the large request runs for tens of milliseconds; the small ones are
+    # submitted right behind it and must be admitted into the free slots
+    # while it runs (continuous batching), not after it drains
+    big = casgemm.gen_g500(17, 16, 3)
+    bigT = big.transpose()
     smalls = [casgemm.gen_g500(8, 4, 10 + i) for i in range(6)]
     with casgemm.Server(slots=3) as srv:
-        b = srv.submit(big, big.transpose())
-        time.sleep(0.05)
+        b = srv.submit(big, bigT)
         ids = [srv.submit(S, S.transpose()) for S in smalls]
         rs = [srv.wait(i, 120.0) for i in ids]
         rb = srv.wait(b, 300.0)
     assert rb["status"] == 0 and all(r["status"] == 0 for r in rs)
-    assert sum(r["t_done"] < rb["t_done"] for r in rs) >= 4
+    assert all(r["t_admit"] < rb["t_done"] for r in rs)
+    assert sum(r["t_done"] < rb["t_done"] for r in rs) >= 1
