@@ -233,6 +233,19 @@ class DeviceCsr:
         self.c = CasCsr(num_row, num_col, nnz, row_ptrs_ptr, cols_ptr, vals_ptr, 4, val_type, 1, 0)
         self._keep = keep
 
+    @property
+    def num_row(self) -> int:
+        return self.c.num_row
+
+    @staticmethod
+    def upload(M: "Csr", device: int = 0) -> "DeviceCsr":
+        """A device copy of host CSR M (torch CUDA tensors, kept alive by the object)."""
+        import torch
+        dev = torch.device("cuda", device)
+        t = [torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in (M.row_ptrs, M.cols, M.vals)]
+        return DeviceCsr(M.num_row, M.num_col, M.nnz, t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(),
+                         M.val_type, keep=t)
+
 
 class Context:
     """A casgemm context on one device (cas_create / cas_destroy)."""
@@ -409,8 +422,11 @@ class Server:
         self.h = h
         self._inputs = {}
 
-    def submit(self, A: Csr, B: Csr) -> int:
-        ca, cb = A.as_cas(), B.as_cas()
+    def submit(self, A, B) -> int:
+        """Queues C = A * B.  A and B are both host Csr, or both DeviceCsr
+        resident on the server's device (uploaded once, served many times)."""
+        ca = A.as_cas() if isinstance(A, Csr) else A.c
+        cb = B.as_cas() if isinstance(B, Csr) else B.c
         rid = ctypes.c_int64()
         st = self.lib.cas_serve_submit(self.h, ctypes.byref(ca), ctypes.byref(cb), ctypes.byref(rid))
         if st != 0:

@@ -24,6 +24,7 @@ struct ServeReq {
   int64_t id = 0;
   cas_csr A{}, B{};
   std::vector<int64_t> cuts;  // row chunk boundaries
+  std::vector<int64_t> a_rp;  // device A split into chunks: A's row pointers, copied at submission
   int64_t flop = 0;
   cas_result res{};
   bool done = false;
@@ -33,12 +34,50 @@ double host_csr_device_bytes(const cas_csr& M) {
   return 8.0 * (double)(M.num_row + 1) + (4.0 + (M.val_type == CAS_VAL_F64 ? 8.0 : 4.0)) * (double)M.num_nnz;
 }
 
+// Row products of a device request (sum over A_i of |B_k|) for its memory
+// bound, and a check of its structure: row pointers that start at 0, end at
+// nnz and do not decrease, columns inside B.  `bad` becomes nonzero on a
+// violation (the row products are then meaningless).
+__global__ void k_serve_row_products(int64_t m, int64_t nnz, const int64_t* __restrict__ arp,
+                                     const int32_t* __restrict__ acol, int64_t brows, const int64_t* __restrict__ brp,
+                                     int64_t* __restrict__ out, int* __restrict__ bad) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && (arp[0] != 0 || arp[m] != nnz)) atomicOr(bad, 1);
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < m; i += warps) {
+    const int64_t s = arp[i], e = arp[i + 1];
+    if (e < s) {
+      if (lane == 0) atomicOr(bad, 2);
+      continue;
+    }
+    long long p = 0;
+    for (int64_t k = s + lane; k < e; k += 32) {
+      const int32_t c = acol[k];
+      if (c < 0 || c >= brows) {
+        atomicOr(bad, 4);
+        continue;
+      }
+      p += brp[c + 1] - brp[c];
+    }
+    p = cas::warp_sum(p);
+    if (lane == 0) out[i] = p;
+  }
+}
+
+// Row pointers of rows [r0, r1) of a device CSR, rebased to start at 0.
+__global__ void k_serve_rebase(int64_t n, const int64_t* __restrict__ src, int64_t base, int64_t* __restrict__ dst) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = src[i] - base;
+}
+
 }  // namespace
 
 struct cas_server {
   cas_server_opts opts{};
   int device = 0;
   std::mutex mu;
+  std::mutex submit_mu;              // device requests: one sizing pass at a time
+  cudaStream_t submit_stream = nullptr;
   std::condition_variable cv;
   std::deque<ServeReq*> pending;
   std::unordered_map<int64_t, ServeReq*> reqs;
@@ -79,10 +118,29 @@ cas_status serve_execute(cas_server* srv, cas_ctx* ctx, ServeReq* r) {
     CAS_CUDA(ctx, cudaMemsetAsync(d_nnz, 0, sizeof(unsigned long long), ctx->stream));
     CAS_CUDA(ctx, cudaMemsetAsync(zero, 0, sizeof(int64_t), ctx->stream));
     std::vector<int64_t> rp;
+    int64_t* d_rp = nullptr;  // device A in chunks: the chunk's rebased row pointers
+    struct RpFree {
+      cas_ctx* c;
+      int64_t** p;
+      ~RpFree() {
+        if (*p) cudaFreeAsync(*p, c->stream);
+      }
+    } rp_free{ctx, &d_rp};
     for (size_t k = 0; k + 1 < r->cuts.size(); ++k) {
       const int64_t r0 = r->cuts[k], r1 = r->cuts[k + 1];
       cas_csr Ac = A;
-      if (r->cuts.size() > 2) {  // a host row slice whose row pointers start at 0
+      if (r->cuts.size() > 2 && A.on_device) {  // a device row slice: row pointers rebased on the device
+        const int64_t base = r->a_rp[(size_t)r0];
+        if (!d_rp) CAS_TRY(dev_alloc(ctx, (void**)&d_rp, sizeof(int64_t) * (size_t)(A.num_row + 1)));
+        k_serve_rebase<<<grid_for(r1 - r0 + 1, 256, ctx->sm_count * 4), 256, 0, ctx->stream>>>(
+            r1 - r0 + 1, A.row_ptrs + r0, base, d_rp);
+        CAS_TRY(check_launch(ctx, "k_serve_rebase"));
+        Ac.num_row = r1 - r0;
+        Ac.num_nnz = r->a_rp[(size_t)r1] - base;
+        Ac.row_ptrs = d_rp;
+        Ac.cols = static_cast<int32_t*>(A.cols) + base;
+        Ac.rats = static_cast<char*>(A.rats) + (f64 ? 8 : 4) * base;
+      } else if (r->cuts.size() > 2) {  // a host row slice whose row pointers start at 0
         rp.resize((size_t)(r1 - r0 + 1));
         for (int64_t i = r0; i <= r1; ++i) rp[(size_t)(i - r0)] = A.row_ptrs[i] - A.row_ptrs[r0];
         Ac.num_row = r1 - r0;
@@ -212,11 +270,18 @@ cas_status cas_serve_create(int device, const cas_server_opts* opts, cas_server*
   }
   srv->device = device;
   if (!srv->opts.dry_run) {
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&srv->submit_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      delete srv;
+      return CAS_ERR_CUDA;
+    }
     for (int i = 0; i < srv->opts.slots; ++i) {
       cas_ctx* c = nullptr;
       const cas_status st = cas_create(device, &c);
       if (st != CAS_OK) {
         for (cas_ctx* x : srv->ctxs) cas_destroy(x);
+        cudaStreamDestroy(srv->submit_stream);
         delete srv;
         return st;
       }
@@ -228,41 +293,104 @@ cas_status cas_serve_create(int device, const cas_server_opts* opts, cas_server*
   return CAS_OK;
 }
 
+// Row products of a device request, with its structure checked on the
+// device; fills rowp (m entries) and, when keep_rp, A's row pointers.
+static cas_status serve_device_rows(cas_server* srv, const cas_csr* A, const cas_csr* B, std::vector<int64_t>& rowp,
+                                    std::vector<int64_t>* a_rp) {
+  std::lock_guard<std::mutex> lk(srv->submit_mu);
+  if (cudaSetDevice(srv->device) != cudaSuccess) return CAS_ERR_CUDA;
+  const int64_t m = A->num_row;
+  cudaStream_t s = srv->submit_stream;
+  int64_t* d_out = nullptr;
+  int* d_bad = nullptr;
+  int bad = 0;
+  cas_status rc = CAS_OK;
+  if (cudaMallocAsync((void**)&d_out, sizeof(int64_t) * (size_t)(m > 0 ? m : 1), s) != cudaSuccess ||
+      cudaMallocAsync((void**)&d_bad, sizeof(int), s) != cudaSuccess) {
+    rc = CAS_ERR_OOM;
+  } else {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, srv->device);
+    cudaMemsetAsync(d_bad, 0, sizeof(int), s);
+    const int64_t blocks = std::min<int64_t>((m * 32 + 255) / 256 + 1, (int64_t)sms * 8);
+    k_serve_row_products<<<(unsigned)blocks, 256, 0, s>>>(m, A->num_nnz, A->row_ptrs,
+                                                          static_cast<const int32_t*>(A->cols), B->num_row,
+                                                          B->row_ptrs, d_out, d_bad);
+    rowp.resize((size_t)m);
+    if (a_rp) a_rp->resize((size_t)m + 1);
+    if (cudaGetLastError() != cudaSuccess ||
+        (m > 0 && cudaMemcpyAsync(rowp.data(), d_out, sizeof(int64_t) * (size_t)m, cudaMemcpyDeviceToHost, s) !=
+                      cudaSuccess) ||
+        (a_rp && cudaMemcpyAsync(a_rp->data(), A->row_ptrs, sizeof(int64_t) * (size_t)(m + 1),
+                                 cudaMemcpyDeviceToHost, s) != cudaSuccess) ||
+        cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      rc = CAS_ERR_CUDA;
+    else if (bad)
+      rc = CAS_ERR_BAD_INPUT;
+  }
+  if (d_out) cudaFreeAsync(d_out, s);
+  if (d_bad) cudaFreeAsync(d_bad, s);
+  cudaStreamSynchronize(s);
+  if (rc == CAS_ERR_CUDA) cudaGetLastError();
+  return rc;
+}
+
 cas_status cas_serve_submit(cas_server* srv, const cas_csr* A, const cas_csr* B, int64_t* id) {
   if (!srv || !A || !B || !id) return CAS_ERR_BAD_INPUT;
   if (basic_checks(nullptr, A, "A") != CAS_OK || basic_checks(nullptr, B, "B") != CAS_OK) return CAS_ERR_BAD_INPUT;
-  if (A->on_device || B->on_device || A->col_bytes != 4 || B->col_bytes != 4 || A->num_col != B->num_row ||
-      A->val_type != B->val_type)
+  const bool dev = A->on_device != 0;
+  if (B->on_device != A->on_device || A->col_bytes != 4 || B->col_bytes != 4 || A->num_col != B->num_row ||
+      A->val_type != B->val_type || (dev && srv->opts.dry_run))
     return CAS_ERR_BAD_INPUT;
-  for (const cas_csr* M : {A, B})
-    if (M->row_ptrs[0] != 0 || M->row_ptrs[M->num_row] != M->num_nnz) return CAS_ERR_BAD_INPUT;
+  if (!dev)
+    for (const cas_csr* M : {A, B})
+      if (M->row_ptrs[0] != 0 || M->row_ptrs[M->num_row] != M->num_nnz) return CAS_ERR_BAD_INPUT;
   ServeReq* r = new (std::nothrow) ServeReq();
   if (!r) return CAS_ERR_OOM;
   r->A = *A;
   r->B = *B;
+  // row products: on the host for host operands, on the device (and the
+  // structure checked there) for resident ones
+  std::vector<int64_t> rowp((size_t)A->num_row);
+  if (dev) {
+    std::vector<int64_t> a_rp;
+    const cas_status st = serve_device_rows(srv, A, B, rowp, &a_rp);
+    if (st != CAS_OK) {
+      delete r;
+      return st;
+    }
+    r->a_rp.swap(a_rp);
+  } else {
+    const int32_t* acol = static_cast<const int32_t*>(A->cols);
+    for (int64_t i = 0; i < A->num_row; ++i) {
+      int64_t p = 0;
+      for (int64_t k = A->row_ptrs[i]; k < A->row_ptrs[i + 1]; ++k) {
+        const int32_t c = acol[k];
+        if (c < 0 || c >= B->num_row) {
+          delete r;
+          return CAS_ERR_BAD_INPUT;
+        }
+        p += B->row_ptrs[c + 1] - B->row_ptrs[c];
+      }
+      rowp[(size_t)i] = p;
+    }
+  }
   // per-row bound: 12 bytes per possible entry of C, 40 per row (the row
-  // pointers of A and C and the pipeline's per-row scratch) and the row's
-  // share of A's device copy; B's copy is fixed
-  const int32_t* acol = static_cast<const int32_t*>(A->cols);
-  const double fixed = 16.0 + host_csr_device_bytes(*B);
+  // pointers of A and C and the pipeline's per-row scratch) and, for host
+  // operands, the row's share of A's device copy; B's copy is fixed.
+  // Resident operands are the caller's memory and are not counted.
+  const double fixed = 16.0 + (dev ? 0.0 : host_csr_device_bytes(*B));
   const double budget = srv->opts.mem_budget;
-  const double ebytes = 4.0 + (A->val_type == CAS_VAL_F64 ? 8.0 : 4.0);
+  const double ebytes = dev ? 0.0 : 4.0 + (A->val_type == CAS_VAL_F64 ? 8.0 : 4.0);
   double total = fixed, chunk = fixed, chunk_max = 0;
   r->cuts.push_back(0);
   std::vector<double> rowb((size_t)A->num_row);
+  const int64_t* arp = dev ? r->a_rp.data() : A->row_ptrs;
   for (int64_t i = 0; i < A->num_row; ++i) {
-    int64_t p = 0;
-    for (int64_t k = A->row_ptrs[i]; k < A->row_ptrs[i + 1]; ++k) {
-      const int32_t c = acol[k];
-      if (c < 0 || c >= B->num_row) {
-        delete r;
-        return CAS_ERR_BAD_INPUT;
-      }
-      p += B->row_ptrs[c + 1] - B->row_ptrs[c];
-    }
+    const int64_t p = rowp[(size_t)i];
     r->flop += p;
-    rowb[(size_t)i] = 12.0 * (double)std::min<int64_t>(p, B->num_col) + 40.0 +
-                      ebytes * (double)(A->row_ptrs[i + 1] - A->row_ptrs[i]);
+    rowb[(size_t)i] = 12.0 * (double)std::min<int64_t>(p, B->num_col) + 40.0 + ebytes * (double)(arp[i + 1] - arp[i]);
     total += rowb[(size_t)i];
   }
   r->res.chunks = 1;
@@ -284,6 +412,7 @@ cas_status cas_serve_submit(cas_server* srv, const cas_csr* A, const cas_csr* B,
     r->res.chunks = (int32_t)(r->cuts.size() - 1);
     r->res.bound = chunk_max;
   }
+  if (r->res.chunks == 1) std::vector<int64_t>().swap(r->a_rp);
   std::lock_guard<std::mutex> lk(srv->mu);
   r->id = srv->next_id++;
   r->res.t_submit = srv->now();
@@ -342,6 +471,7 @@ void cas_serve_destroy(cas_server* srv) {
   srv->cv.notify_all();
   for (std::thread& t : srv->workers) t.join();
   for (cas_ctx* c : srv->ctxs) cas_destroy(c);
+  if (srv->submit_stream) cudaStreamDestroy(srv->submit_stream);
   for (auto& kv : srv->reqs) {
     cas_csr& C = kv.second->res.C;
     if (C.owned && !C.on_device) {

@@ -288,10 +288,17 @@ cas_status cas_batch_run(cas_ctx *ctx, cas_accum accum, cas_job *jobs, int64_t n
  * scratch), computed at submission from the row products.  Admitted requests
  * run concurrently on the device, and later arrivals join as slots and
  * memory free up.  A request whose bound exceeds the whole budget runs in row
- * chunks that each fit.  Inputs are host CSRs (col_bytes 4); the server
- * reads a request's A and B until it completes, so the caller keeps those
- * arrays alive until then.  Times are seconds on the server's monotonic
- * clock (cas_serve_clock). */
+ * chunks that each fit.  Inputs are CSRs with col_bytes 4, both on the host
+ * or both resident on the server's device (on_device 1): a caller that
+ * serves the same matrices again and again uploads each once and submits
+ * the device copies, so no request copies its operands.  For resident
+ * operands the bound leaves out A's and B's copies (they are the caller's
+ * memory), and submission computes the row products on the device and checks
+ * the structure there (row pointers from 0 to nnz, columns inside B;
+ * CAS_ERR_BAD_INPUT otherwise).  The server reads a request's A and B until
+ * it completes, so the caller keeps those arrays alive and unchanged until
+ * then.  Times are seconds on the server's monotonic clock
+ * (cas_serve_clock). */
 typedef struct cas_server cas_server;
 
 typedef struct {

@@ -151,3 +151,55 @@ def test_small_requests_pass_a_large_one():
     assert rb["status"] == 0 and all(r["status"] == 0 for r in rs)
     assert all(r["t_admit"] < rb["t_done"] for r in rs)
     assert sum(r["t_done"] < rb["t_done"] for r in rs) >= 1
+
+
+@pytest.mark.gpu
+def test_resident_operands_equal_alone():
+    """Operands uploaded once and kept on the device: several requests name
+    the same resident matrices, mixed with host requests; each result equals
+    the same product alone.  A chunked resident request (row pointers rebased
+    on the device) equals its product too."""
+    if not has_gpu():
+        pytest.skip("no CUDA device")
+    reqs = requests(6, 3)
+    dev = [(casgemm.DeviceCsr.upload(A), casgemm.DeviceCsr.upload(B)) for A, B in reqs]
+    order = [0, 1, 2, 0, 3, 1, 4, 5, 0, 2]
+    with casgemm.Server(slots=3, keep_output=True) as srv:
+        ids = [srv.submit(*dev[k]) for k in order] + [srv.submit(*reqs[1])]
+        res = [srv.wait(i, 120.0) for i in ids]
+    for r, k in zip(res, order + [1]):
+        A, B = reqs[k]
+        rp, cols, vals, flop, d = alone(A, B)
+        assert r["status"] == 0
+        assert r["flop"] == flop and r["nnz_c"] == len(cols) and r["digest"] == d
+        np.testing.assert_array_equal(r["C"].row_ptrs, rp)
+        np.testing.assert_array_equal(r["C"].vals, vals)
+    A = casgemm.gen_g500(11, 8, 9)
+    B = A.transpose()
+    dA, dB = casgemm.DeviceCsr.upload(A), casgemm.DeviceCsr.upload(B)
+    budget = 16.0 + (bound_of(A, B) - 16.0 - 8.0 * (B.num_row + 1) - 12.0 * B.nnz) / 6
+    with casgemm.Server(slots=2, mem_budget=budget, keep_output=True) as srv:
+        r = srv.wait(srv.submit(dA, dB), 120.0)
+    rp, cols, vals, flop, d = alone(A, B)
+    assert r["status"] == 0 and r["chunks"] >= 5
+    assert r["digest"] == d and r["nnz_c"] == len(cols) and r["flop"] == flop
+    np.testing.assert_array_equal(r["C"].row_ptrs, rp)
+    np.testing.assert_array_equal(r["C"].cols.astype(np.int64), cols)
+    np.testing.assert_array_equal(r["C"].vals, vals)
+
+
+@pytest.mark.gpu
+def test_resident_operands_checked_at_submission():
+    """A resident request whose columns leave B is refused at submission."""
+    if not has_gpu():
+        pytest.skip("no CUDA device")
+    import torch
+    A = casgemm.gen_g500(8, 4, 1)
+    B = A.transpose()
+    bad_cols = A.cols.copy()
+    bad_cols[5] = B.num_row + 7
+    t = [torch.from_numpy(x).cuda() for x in (A.row_ptrs, bad_cols, A.vals)]
+    dA = casgemm.DeviceCsr(A.num_row, A.num_col, A.nnz, t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(), keep=t)
+    with casgemm.Server(slots=1) as srv:
+        with pytest.raises(casgemm.CasError):
+            srv.submit(dA, casgemm.DeviceCsr.upload(B))
