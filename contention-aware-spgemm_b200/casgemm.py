@@ -147,6 +147,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                              ctypes.POINTER(CasRuntime)]),
         "cas_csr_free": (I32, [P, ctypes.POINTER(CasCsr)]),
         "cas_csr_digest": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(ctypes.c_uint64), P]),
+        "cas_csr_transpose": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr)]),
         "cas_batch_run": (I32, [P, I32, ctypes.POINTER(CasJob), I64, I32, D, ctypes.POINTER(CasBatchStats)]),
         "cas_serve_create": (I32, [ctypes.c_int, ctypes.POINTER(CasServerOpts), ctypes.POINTER(P)]),
         "cas_serve_submit": (I32, [P, ctypes.POINTER(CasCsr), ctypes.POINTER(CasCsr), ctypes.POINTER(I64)]),
@@ -361,6 +362,32 @@ class Context:
         self._check(self.lib.cas_spgemm(self.h, ACCUM[accum], ctypes.byref(A.c), ctypes.byref(B.c),
                                         ctypes.byref(cc), ctypes.byref(rt)))
         return cc, rt.as_dict()
+
+    def transpose(self, A) -> Csr:
+        """B = A^T computed on the device (cas_csr_transpose), returned on the host."""
+        ca = A.as_cas() if isinstance(A, Csr) else A.c
+        cb = CasCsr()
+        cb.on_device = 0
+        self._check(self.lib.cas_csr_transpose(self.h, ctypes.byref(ca), ctypes.byref(cb)))
+        try:
+            n, nnz = cb.num_row, cb.num_nnz
+            rp = np.ctypeslib.as_array(ctypes.cast(cb.row_ptrs, ctypes.POINTER(ctypes.c_int64)), (n + 1,)).copy()
+            vt, vdt = (ctypes.c_double, np.float64) if cb.val_type == VAL_F64 else (ctypes.c_int32, np.int32)
+            cols = (np.ctypeslib.as_array(ctypes.cast(cb.cols, ctypes.POINTER(ctypes.c_int32)), (nnz,)).copy()
+                    if nnz else np.zeros(0, np.int32))
+            vals = (np.ctypeslib.as_array(ctypes.cast(cb.rats, ctypes.POINTER(vt)), (nnz,)).copy()
+                    if nnz else np.zeros(0, vdt))
+        finally:
+            self.lib.cas_csr_free(self.h, ctypes.byref(cb))
+        return Csr(n, A.num_row, rp, cols, vals)
+
+    def transpose_device(self, A) -> CasCsr:
+        """B = A^T on the device, owned by the library (release with :meth:`free`)."""
+        ca = A.as_cas() if isinstance(A, Csr) else A.c
+        cb = CasCsr()
+        cb.on_device = 1
+        self._check(self.lib.cas_csr_transpose(self.h, ctypes.byref(ca), ctypes.byref(cb)))
+        return cb
 
     def free(self, cc: CasCsr):
         self._check(self.lib.cas_csr_free(self.h, ctypes.byref(cc)))

@@ -1437,6 +1437,7 @@ cas_status cas_hybacc_numc(cas_ctx* ctx, const cas_csr* A, const cas_csr* B, con
 // ============================================= digests and batches of products
 #include "cas_batch.cu"
 #include "cas_serve.cu"
+#include "cas_transpose.cu"
 
 // ===================================================== scan without allocation
 // cas_scan_noalloc: the same exclusive scan as cas_scan, for callers that must

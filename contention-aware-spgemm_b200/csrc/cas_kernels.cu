@@ -1511,14 +1511,19 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   static_assert(NG <= BLOCK && NCH <= BLOCK && NB % (2 * BLOCK) == 0, "one count per thread in the scans");
   static_assert(TS >= CAP + CAP / 4, "hash of deferred rows: load at most 0.8");
   extern __shared__ __align__(16) uint8_t smem[];
-  uint32_t* skey = reinterpret_cast<uint32_t*>(smem);
+  // REGK puts place_of first: everything after it up to the byte table
+  // (and the byte table too, when the value pass walks B rows) is dead by
+  // the value pass and then holds the row's values at their places
+  uint16_t* place_of = REGK ? reinterpret_cast<uint16_t*>(smem)
+                            : reinterpret_cast<uint16_t*>(smem + size_t(CAP) * 6);  // per product: its column's place
+  uint32_t* skey = reinterpret_cast<uint32_t*>(REGK ? smem + size_t(CAP) * 2 : smem);
   uint16_t* sidx = reinterpret_cast<uint16_t*>(skey + CAP);
-  uint16_t* place_of = sidx + CAP;                             // per product: its column's place in the row
-  uint32_t* bcnt = reinterpret_cast<uint32_t*>(place_of + CAP);  // NB 16-bit counters
+  uint32_t* bcnt = reinterpret_cast<uint32_t*>(smem + size_t(CAP) * 8);  // NB 16-bit counters
   uint32_t* ccnt = bcnt + NB / 2;                              // NCH head counts / offsets
   uint32_t* hmw = ccnt + NCHP;                                 // NCH head masks
   uint8_t* segof = reinterpret_cast<uint8_t*>(hmw + NCHP);
   StageB<VIn>& sg = *reinterpret_cast<StageB<VIn>*>(segof + ((CAP + 15) & ~15));
+  static_assert(CAP % 32 == 0, "8-byte alignment of the staged values after place_of");
   __shared__ long long s_tick, s_off;
   __shared__ int s_huge, s_hlast;
   __shared__ uint32_t s_hkb;       // first column of the huge bucket
@@ -1565,7 +1570,7 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   // the shared arena) and published; all go to the radix-sort ESC kernel
   auto defer = [&]() {
     if (FUSED) {
-      uint32_t* tab = skey;
+      uint32_t* tab = reinterpret_cast<uint32_t*>(smem);
       __syncthreads();
       for (int i = threadIdx.x; i < TS; i += BLOCK) tab[i] = kEmptyKey;
       __syncthreads();
@@ -1805,8 +1810,17 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
     c0 = crp[r];
     __syncthreads();
   }
+  // REGK: values staged in shared memory at their places and copied out in
+  // order, when they fit the dead part of the arena (with the byte table
+  // when the value pass walks B rows)
+  const bool seg_walk = REGK && n >= 32 * (int)(ae - as);
+  const size_t dead = size_t(CAP) * 6 + size_t(NB) * 2 + size_t(NCHP) * 8 + (seg_walk ? ((CAP + 15) & ~15) : 0);
+  const bool stage = REGK && (size_t)nz * sizeof(AT) <= dead;
+  AT* sval = reinterpret_cast<AT*>(skey);
+  if (stage && threadIdx.x == 0) s_hlast = 0x7FFFFFFF;  // reused: the huge bucket's first place
+  __syncthreads();
   // sorted order: each distinct column to C; the huge bucket's sums; a zero
-  // where several products will add
+  // where several products will add (staged values are zeroed below)
   for (int c = warp; c < nch; c += NW) {
     const int t = c * 32 + lane;
     const unsigned m = hmw[c];
@@ -1815,12 +1829,25 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
       if (run < nz) {
         const uint32_t key = skey[t];
         ccol[c0 + run] = (int32_t)key;
-        if (sidx[t] == kFromSum) cval[c0 + run] = hsum[key - s_hkb];
-        else if (t + 1 < n && !head_at(t + 1) && sidx[t + 1] != kNoProduct) cval[c0 + run] = AT(0);
+        if (sidx[t] == kFromSum) {
+          cval[c0 + run] = hsum[key - s_hkb];
+          if (stage) atomicMin(&s_hlast, run);
+        } else if (!stage && t + 1 < n && !head_at(t + 1) && sidx[t + 1] != kNoProduct) {
+          cval[c0 + run] = AT(0);
+        }
       }
     }
   }
   __syncthreads();
+  int hp0 = 0, hp1 = 0;  // places of the huge bucket's columns, written above from its sums
+  if (stage) {
+    if (huge) {
+      hp0 = s_hlast;
+      hp1 = hp0 + hpre[kHugeWidth / 32];
+    }
+    for (int i = threadIdx.x; i < (int)nz; i += BLOCK) sval[i] = AT(0);
+    __syncthreads();
+  }
   // product order: a_ik * b_kj to its place (REGK: a warp per B row when
   // the chunk's B rows average at least 32 products)
   auto put = [&](VIn av, VIn bv, int p) {
@@ -1830,8 +1857,24 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
     if (o & kShared) Acc<VIn>::atomic_add(&cval[c0 + (o & ~kShared)], v);
     else cval[c0 + o] = v;
   };
-  if (REGK && n >= 32 * (int)(ae - as)) expand_values_seg<BLOCK, VIn>(B, (int)(ae - as), sg, put);
-  else expand_values<BLOCK, VIn>(B, n, sg, segof, put);
+  auto put_staged = [&](VIn av, VIn bv, int p) {
+    const uint16_t o = place_of[p];
+    if (o == kSkip) return;
+    const AT v = Acc<VIn>::mul(av, bv);
+    if (o & kShared) atomic_add_sh(&sval[o & ~kShared], v);
+    else sval[o] = v;
+  };
+  if (stage) {
+    if (seg_walk) expand_values_seg<BLOCK, VIn>(B, (int)(ae - as), sg, put_staged);
+    else expand_values<BLOCK, VIn>(B, n, sg, segof, put_staged);
+    __syncthreads();
+    for (int i = threadIdx.x; i < (int)nz; i += BLOCK)
+      if (i < hp0 || i >= hp1) cval[c0 + i] = sval[i];
+  } else if (seg_walk) {
+    expand_values_seg<BLOCK, VIn>(B, (int)(ae - as), sg, put);
+  } else {
+    expand_values<BLOCK, VIn>(B, n, sg, segof, put);
+  }
   if (!FUSED && threadIdx.x == 0 && distinct != nz)
     dev_report(st, distinct > nz ? kDevRowOverflow : kDevRowUnderflow, 16, r);
 }

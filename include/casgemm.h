@@ -218,6 +218,22 @@ cas_status cas_spgemm(cas_ctx *ctx, cas_accum accum, const cas_csr *A, const cas
  * them); this is safe from any thread. */
 cas_status cas_csr_free(cas_ctx *ctx, cas_csr *C);
 
+/* ---- the second input: B = Aᵀ on the device -------------------------------
+ *
+ * B = Aᵀ made on the device from A, so a caller with A alone needs no
+ * transposed file.  Replaces the reference's trpl_transpose
+ * (src/mm/mm_utils.c:742-754), which swaps every triple's row and column and
+ * sorts the triples by (row, column) before txt_transpose (:851-862) writes
+ * them to <dataset>.trs.mtx for the drivers to read.  A is a host CSR (int32
+ * or int64 columns) or a device CSR (col_bytes 4), checked on the device
+ * (CAS_ERR_BAD_INPUT for row pointers or columns out of range).  B is
+ * allocated by the library: on the device when B->on_device is 1 on entry,
+ * else in host memory; col_bytes 4, A's value type; release it with
+ * cas_csr_free.  Rows of B are sorted by column, and duplicate (row, column)
+ * entries of A keep their order, so B equals the host's stable
+ * counting-sort transpose entry for entry. */
+cas_status cas_csr_transpose(cas_ctx *ctx, const cas_csr *A, cas_csr *B);
+
 /* ---- digests of a product ------------------------------------------------
  *
  * A 64-bit digest of a CSR C that depends on every row's entries in order,

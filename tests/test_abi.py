@@ -34,7 +34,8 @@ def test_every_declared_symbol_is_exported(header):
 def test_expected_entry_points_declared():
     names = set(declared(HEADERS[0]))
     for n in ("cas_create", "cas_destroy", "cas_spgemm", "cas_flp_populate", "cas_scan", "cas_hash_symb",
-              "cas_hash_numc", "cas_hsersc_numc", "cas_hybacc_numc", "cas_csr_free", "cas_scan_noalloc"):
+              "cas_hash_numc", "cas_hsersc_numc", "cas_hybacc_numc", "cas_csr_free", "cas_scan_noalloc",
+              "cas_csr_transpose", "cas_serve_submit"):
         assert n in names
 
 

@@ -126,3 +126,23 @@ def test_driver_matches_reference_log(tmp_path, algo):
                        env=env, timeout=300)
     assert q.returncode == 0, q.stderr
     assert set(verify_triples(q.stdout)) == set(verify_triples(ref))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("algo", ["hybacc"])
+def test_driver_without_transposed_file(tmp_path, algo):
+    """With no <dataset>.trs.mtx, B = A^T is made on the device and the
+    driver prints the reference's VERIFYRESULT triple all the same."""
+    ds = tmp_path / "dataset"
+    subprocess.run([os.path.join(BIN, "cas_gen"), "g500", "12", "8"], check=True, capture_output=True,
+                   env=dict(os.environ, CAS_DATASET_DIR=str(ds)))
+    (ds / "g500_12_8.trs.mtx").unlink()
+    env = dict(os.environ, CAS_RUN_NUM="2", CAS_VERIFY="1")
+    p = subprocess.run([os.path.join(BIN, ALGOS[algo]), "g500_12_8"], cwd=tmp_path, capture_output=True, text=True,
+                       env=env, timeout=300)
+    assert p.returncode == 0, p.stderr
+    assert "made on the device" in p.stderr
+    ref = open(os.path.join(GOLDEN, f"driver_{algo}_g500_12_8.log")).read()
+    assert set(verify_triples(p.stdout)) == set(verify_triples(ref))
+    assert dict(summary_fields(p.stdout))["flop_cnt"] == dict(summary_fields(ref))["flop_cnt"]
+

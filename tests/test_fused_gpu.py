@@ -251,23 +251,43 @@ def test_index_form_many_shared_columns(ctx, per_b):
         ctx.set_tuning(**saved)
 
 
+def _hot_long_rows(seed=8, ncol=3000, per_row=80, blen=40, hot=2):
+    """Fused rows (80 A entries of B rows with 40 columns each: 3200
+    products) whose B rows all hold the hot columns 0..hot-1, so one bucket
+    gets 160 products over 2 columns (summed densely), while the B rows are
+    long enough for the value pass to walk them a warp per row."""
+    rng = np.random.default_rng(seed)
+    n_rows, n_mid = 30, 300
+    r = np.repeat(np.arange(n_rows), per_row)
+    c = np.concatenate([rng.choice(n_mid, per_row, replace=False) for _ in range(n_rows)])
+    A = from_coo(n_rows, n_mid, r, c)
+    bc = [np.concatenate([np.arange(hot), rng.choice(np.arange(hot, ncol), blen - hot, replace=False)])
+          for _ in range(n_mid)]
+    B = from_coo(n_mid, ncol, np.repeat(np.arange(n_mid), blen), np.concatenate(bc))
+    return A, B
+
+
 def _register_form_cases():
     er = casgemm.gen_er(13, 32, 7)
     er_wide = casgemm.gen_er(12, 40, 3)   # rows of 4801..6144 products: the 6144 bin
     g500 = casgemm.gen_g500(12, 16, 5)   # short B rows: the product-order value pass
     hotA, hotB = hot_column_matrix(per_row=120, hot=2)
+    longA, longB = _hot_long_rows()
     return [("er_s13_ef32", er, er.transpose()), ("er_s12_ef40", er_wide, er_wide.transpose()),
             ("g500_s12_ef16", g500, g500.transpose()), ("hot_columns", hotA, hotB),
-            ("g500_int", with_int_values(g500, 9), with_int_values(g500, 9).transpose())]
+            ("g500_int", with_int_values(g500, 9), with_int_values(g500, 9).transpose()),
+            ("hot_long_rows", longA, longB)]
 
 
 @pytest.mark.parametrize("fuse", [True, False])
-@pytest.mark.parametrize("case", range(5), ids=["er_s13_ef32", "er_s12_ef40", "g500_s12_ef16", "hot_columns",
-                                                  "g500_int"])
+@pytest.mark.parametrize("case", range(6), ids=["er_s13_ef32", "er_s12_ef40", "g500_s12_ef16", "hot_columns",
+                                                  "g500_int", "hot_long_rows"])
 def test_register_form_matches_oracle(ctx, case, fuse):
     """esc_form 2: the index form with each thread's keys held in registers
-    between the histogram and the scatter, and (for long B rows) a warp per B
-    row in the value pass; fused rows and the 4800 / 6144 ESC bins."""
+    between the histogram and the scatter, (for long B rows) a warp per B
+    row in the value pass, and values staged in shared memory at their
+    places and copied out in order; fused rows and the 4800 / 6144 ESC
+    bins, with a bucket of hub columns summed densely among them."""
     name, A, B = _register_form_cases()[case]
     ref = oracle.oracle_spgemm(A, B, "hybacc")
     saved = ctx.get_tuning()
