@@ -450,6 +450,8 @@ def main():
                     help="pick the row routing with casgemm.Autotuner (cached in CACHE.json) before timing")
     ap.add_argument("--esc-form", type=int, default=None, choices=[0, 1, 2],
                     help="bucketed ESC kernel form (cas_tuning.esc_form); default: the library's")
+    ap.add_argument("--assemble", action="store_true",
+                    help="N > 1: assemble C's row shards on rank 0 after the timed steps (reported, not timed)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -551,6 +553,33 @@ def main():
     # row digests of one product for the parity check against the reference
     cc, _ = ctx.spgemm_device(dA, dB, args.accum)
     _, gpu_rows = ctx.digest(cc, rows=True)
+    assembly = None
+    if dist and args.assemble:
+        # C's row shards assembled on rank 0 (all-gather of the shard sizes,
+        # then point-to-point NCCL transfers), timed on the device, max over
+        # ranks; rank 0 checks the assembled rows' digests against the shards'
+        rp_t, col_t, val_t = casgemm.device_tensors(cc)
+        torch.cuda.synchronize()
+        dist.barrier()
+        ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ea.record()
+        got = casgemm.gather_shards(rp_t, col_t, val_t, r0, r1, r_end)
+        eb.record()
+        torch.cuda.synchronize()
+        t = torch.tensor([ea.elapsed_time(eb)], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        shard_rows = [None] * world
+        dist.all_gather_object(shard_rows, gpu_rows)
+        if rank == 0:
+            full = casgemm.CasCsr(r_end, B.num_col, int(got[0][-1]), got[0].data_ptr(),
+                                  got[1].data_ptr(), got[2].data_ptr(), 4, 0, 1, 0)
+            _, rows_full = ctx.digest(full, rows=True)
+            match = bool(np.array_equal(rows_full, np.concatenate(shard_rows)))
+            assembly = {"ms": round(float(t.item()), 3), "nnz": int(got[0][-1]),
+                        "bytes": 8.0 * (r_end + 1) + 12.0 * float(got[0][-1]), "row_digests_match": match,
+                        "how": "all-gather of shard sizes, point-to-point NCCL sends of columns, values and "
+                               "row pointers to rank 0"}
+        del got, rp_t, col_t, val_t
     ctx.free(cc)
 
     # per-kernel times for the roofline: extra steps with the bins run one at
@@ -620,6 +649,8 @@ def main():
         "gpu_launches": launches_total,
         "clocks": clocks,
     }
+    if assembly is not None:
+        line["assembly"] = assembly
 
     # end to end through the public C ABI with pinned host buffers: H2D of A and
     # B, the product, D2H of C into host memory, every step

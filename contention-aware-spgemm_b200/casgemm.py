@@ -720,6 +720,84 @@ def row_shard(prefix: np.ndarray, rank: int, world: int, r_end: Optional[int] = 
     return r0, r1
 
 
+class _DeviceView:
+    """A device array as __cuda_array_interface__ (zero copy, for torch.as_tensor)."""
+
+    def __init__(self, ptr: int, count: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": typestr, "data": (ptr, False), "version": 3}
+
+
+def device_tensors(cc: CasCsr):
+    """torch views (no copy) of a device CSR's row pointers, columns and
+    values, e.g. a C the library allocated; valid until it is freed."""
+    import torch
+
+    def view(ptr, n, typestr, dtype):
+        if n == 0:
+            return torch.empty(0, dtype=dtype, device="cuda")
+        return torch.as_tensor(_DeviceView(ptr, n, typestr), device="cuda")
+
+    vt = ("<f8", torch.float64) if cc.val_type == VAL_F64 else ("<i8", torch.int64)
+    return (view(cc.row_ptrs, cc.num_row + 1, "<i8", torch.int64), view(cc.cols, cc.num_nnz, "<i4", torch.int32),
+            view(cc.rats, cc.num_nnz, *vt))
+
+
+def gather_shards(rp, cols, vals, r0: int, r1: int, num_row: int, root: int = 0):
+    """Assembles the row shards of C from every rank on `root`.
+
+    Each rank passes its shard, rows [r0, r1) of C, as torch tensors: row
+    pointers starting at 0 (r1 - r0 + 1 entries), columns and values.  The
+    ranks all-gather (r0, r1, nnz) of every shard; the root then receives
+    each other rank's columns, values and row pointers by point-to-point
+    transfers (NCCL over NVLink for CUDA tensors, gloo for host tensors) into
+    its slice of C, and shifts the row pointers by the nnz of the shards
+    before it.  Shards must cover [0, num_row) in rank order.  Returns (rp,
+    cols, vals) of the whole C on the root and None elsewhere."""
+    import torch
+    import torch.distributed as dist
+    world, rank = dist.get_world_size(), dist.get_rank()
+    dev = cols.device
+    meta = torch.tensor([r0, r1, int(rp[-1]) if len(rp) else 0], dtype=torch.int64, device=dev)
+    allm = [torch.empty_like(meta) for _ in range(world)]
+    dist.all_gather(allm, meta)
+    allm = [tuple(int(x) for x in m.tolist()) for m in allm]
+    if [m[0] for m in allm] != sorted(m[0] for m in allm) or allm[0][0] != 0 or allm[-1][1] != num_row or \
+            any(allm[q][1] != allm[q + 1][0] for q in range(world - 1)):
+        raise ValueError("row shards must cover [0, num_row) in rank order")
+    offs = [0]
+    for m in allm:
+        offs.append(offs[-1] + m[2])
+    if rank != root:
+        reqs = [dist.isend(rp.contiguous(), root)]
+        if allm[rank][2] > 0:
+            reqs += [dist.isend(cols.contiguous(), root), dist.isend(vals.contiguous(), root)]
+        for r in reqs:
+            r.wait()
+        return None
+    C_rp = torch.empty(num_row + 1, dtype=torch.int64, device=dev)
+    C_cols = torch.empty(offs[-1], dtype=cols.dtype, device=dev)
+    C_vals = torch.empty(offs[-1], dtype=vals.dtype, device=dev)
+    parts, reqs = [], []
+    for q, (a0, a1, n) in enumerate(allm):
+        if q == root:
+            parts.append((q, rp))
+            C_cols[offs[q]:offs[q] + n] = cols
+            C_vals[offs[q]:offs[q] + n] = vals
+            continue
+        buf = torch.empty(a1 - a0 + 1, dtype=torch.int64, device=dev)
+        reqs.append(dist.irecv(buf, q))
+        parts.append((q, buf))
+        if n > 0:
+            reqs.append(dist.irecv(C_cols[offs[q]:offs[q] + n], q))
+            reqs.append(dist.irecv(C_vals[offs[q]:offs[q] + n], q))
+    for r in reqs:
+        r.wait()
+    for q, part in parts:
+        a0, a1, _ = allm[q]
+        C_rp[a0:a1 + 1] = part + offs[q]
+    return C_rp, C_cols, C_vals
+
+
 def slice_rows(A: Csr, r0: int, r1: int) -> Csr:
     """Rows [r0, r1) of A as a CSR of its own (views, no copy of columns/values)."""
     s, e = int(A.row_ptrs[r0]), int(A.row_ptrs[r1])
