@@ -56,7 +56,7 @@ class CasStats(ctypes.Structure):
         ("numc_bin_bytes", ctypes.c_double * 13), ("numc_bin_flop", ctypes.c_int64 * 13),
         ("esc_overflow_rows", ctypes.c_int64), ("esc_overflow_ms", ctypes.c_double),
         ("fused_rows", ctypes.c_int64), ("fused_flop", ctypes.c_int64), ("fused_bytes", ctypes.c_double),
-        ("fused_ms", ctypes.c_double), ("d2h_direct_bytes", ctypes.c_double),
+        ("fused_ms", ctypes.c_double), ("d2h_direct_bytes", ctypes.c_double), ("split_rows", ctypes.c_int64),
     ]
 
 
@@ -108,6 +108,7 @@ class CasTuning(ctypes.Structure):
     _fields_ = [
         ("acc_thres", ctypes.c_double), ("fusion", ctypes.c_int32), ("fused_min_products", ctypes.c_int32),
         ("esc_max_products", ctypes.c_int32), ("hash_max_nnz", ctypes.c_int32), ("esc_form", ctypes.c_int32),
+        ("heavy_split", ctypes.c_int32),
     ]
 
     def as_dict(self):
@@ -297,7 +298,8 @@ class Context:
             raise ValueError(f"unknown tuning knobs {sorted(unknown)}")
         cur.update(kw)
         t = CasTuning(float(cur["acc_thres"]), int(cur["fusion"]), int(cur["fused_min_products"]),
-                      int(cur["esc_max_products"]), int(cur["hash_max_nnz"]), int(cur["esc_form"]))
+                      int(cur["esc_max_products"]), int(cur["hash_max_nnz"]), int(cur["esc_form"]),
+                      int(cur["heavy_split"]))
         self._check(self.lib.cas_set_tuning(self.h, ctypes.byref(t)))
 
     def set_fusion(self, on: bool):
@@ -323,7 +325,7 @@ class Context:
             "numc_bin_flop": dict(zip(NUMC_BINS, list(s.numc_bin_flop))),
             "esc_overflow_rows": s.esc_overflow_rows, "esc_overflow_ms": s.esc_overflow_ms,
             "fused_rows": s.fused_rows, "fused_flop": s.fused_flop, "fused_bytes": s.fused_bytes,
-            "fused_ms": s.fused_ms, "d2h_direct_bytes": s.d2h_direct_bytes,
+            "fused_ms": s.fused_ms, "d2h_direct_bytes": s.d2h_direct_bytes, "split_rows": s.split_rows,
         }
 
     def spgemm(self, A, B, accum: str = "hybacc", col_bytes: int = 4) -> Result:
@@ -585,7 +587,7 @@ class Autotuner:
         if not cfg:
             return False
         self.ctx.set_tuning(**{k: cfg[k] for k in ("acc_thres", "fusion", "fused_min_products",
-                                                    "esc_max_products", "hash_max_nnz", "esc_form")
+                                                    "esc_max_products", "hash_max_nnz", "esc_form", "heavy_split")
                                if k in cfg})
         return True
 

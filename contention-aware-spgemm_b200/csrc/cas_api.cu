@@ -69,6 +69,7 @@ struct cas_ctx {
   bool profile = false;
   bool fuse = true;                        // fused ESC rows (no symbolic pass) in cas_spgemm
   int fused_lo = (int)cas::kFusedLo;       // fused rows: more products than this (up to kFusedHi)
+  bool heavy_split = true;                 // dense rows of 2^18 products or more split across blocks
   int esc_form = 1;                        // bucketed ESC of rows over 4096 products (fused rows included):
                                            // 1 index form (k_numc_esc_idx), 0 k_numc_esc_msd, 2 the index
                                            // form with the keys in registers between its two key passes
@@ -240,6 +241,8 @@ cas_status setup_numc_kernels(cas_ctx* ctx) {
   CAS_TRY(allow_smem(ctx, k_numc_hash<256, 11, VIn>, smem_numc_hash<256, 11, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_hash<512, 13, VIn>, smem_numc_hash<512, 13, VIn>()));
   CAS_TRY(allow_smem(ctx, k_numc_dense<512, VIn>, smem_numc_dense<512, VIn>()));
+  CAS_TRY(allow_smem(ctx, k_dense_setup<512, VIn>, smem_numc_dense<512, VIn>()));
+  CAS_TRY(allow_smem(ctx, k_dense_acc<512, VIn>, smem_numc_dense<512, VIn>()));
   return CAS_OK;
 }
 
@@ -905,11 +908,67 @@ void launch_esc_bin(int esc_form, int64_t n, cudaStream_t s, const int32_t* rows
       rows, A, B, b_sorted, crp, ccol, cval, ovf, ovf_count, st, Fused{});
 }
 
+// The heaviest dense rows over several blocks (k_dense_setup, then
+// k_dense_acc; see cas_kernels.cu), on stream s, with scratch allocated and
+// freed on s: the slice bitmaps (64 KiB per row and slice), the per-row
+// plan and the product prefix of every A entry.
+constexpr int64_t kSplitScratch = int64_t(8) << 30;  // at most 8 GiB of slice bitmaps
+
+template <typename VIn>
+cas_status launch_heavy_split(cas_ctx* ctx, Call& c, const int32_t* rows, int64_t n, const int64_t* crp, int32_t* ccol,
+                              typename cas::Acc<VIn>::T* cval, cudaStream_t s) {
+  using namespace cas;
+  HeavyPlan hp{};
+  hp.rows = rows;
+  hp.n = n;
+  hp.max_slices = (int)((c.ncol + kRankCols - 1) / kRankCols);
+  std::vector<void*> tmp;
+  auto alloc = [&](void** p, size_t bytes) -> cas_status {
+    cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, s);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(ctx, e == cudaErrorMemoryAllocation ? CAS_ERR_OOM : CAS_ERR_CUDA,
+                     "device allocation of %zu bytes for the split rows failed", bytes);
+    }
+    tmp.push_back(*p);
+    return CAS_OK;
+  };
+  cas_status rc = [&]() -> cas_status {
+    CAS_TRY(alloc((void**)&hp.bits, (size_t)n * hp.max_slices * (kRankCols / 8)));
+    CAS_TRY(alloc((void**)&hp.slice_base, sizeof(int64_t) * (size_t)n * hp.max_slices));
+    CAS_TRY(alloc((void**)&hp.lo, sizeof(int64_t) * (size_t)n));
+    CAS_TRY(alloc((void**)&hp.hi, sizeof(int64_t) * (size_t)n));
+    CAS_TRY(alloc((void**)&hp.nslices, sizeof(int32_t) * (size_t)n));
+    CAS_TRY(alloc((void**)&hp.products, sizeof(int64_t) * (size_t)n));
+    CAS_TRY(alloc((void**)&hp.nparts, sizeof(int64_t) * (size_t)n));
+    CAS_TRY(alloc((void**)&hp.parts, sizeof(int64_t) * (size_t)(n + 1)));
+    CAS_TRY(alloc((void**)&hp.apre, sizeof(int64_t) * (size_t)(c.A.nnz > 0 ? c.A.nnz : 1)));
+    CAS_TRY(alloc((void**)&hp.ticket, sizeof(unsigned long long)));
+    CAS_CUDA(ctx, cudaMemsetAsync(hp.ticket, 0, sizeof(unsigned long long), s));
+    k_dense_setup<512, VIn><<<(unsigned)n, 512, smem_numc_dense<512, VIn>(), s>>>(
+        hp, c.A.csr, c.B.csr, c.ncol, c.b_sorted ? 1 : 0, crp, ccol, cval, c.dbits, c.dslot, ctx->d_status);
+    CAS_TRY(check_launch(ctx, "k_dense_setup"));
+    k_scan_one_block<<<1, 1024, 0, s>>>(hp.nparts, n, hp.parts);
+    CAS_TRY(check_launch(ctx, "k_scan_one_block"));
+    int per_sm = 0;
+    CAS_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_acc<512, VIn>, 512,
+                                                                smem_numc_dense<512, VIn>()));
+    const int grid = std::max(1, per_sm) * ctx->sm_count;
+    k_dense_acc<512, VIn><<<grid, 512, smem_numc_dense<512, VIn>(), s>>>(hp, c.A.csr, c.B.csr, crp, cval,
+                                                                       ctx->d_status);
+    CAS_TRY(check_launch(ctx, "k_dense_acc"));
+    return CAS_OK;
+  }();
+  for (void* p : tmp) cudaFreeAsync(p, s);
+  return rc;
+}
+
 template <typename VIn>
 cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* ccol, void* cval_v) {
   using namespace cas;
   using AT = typename Acc<VIn>::T;
   AT* cval = static_cast<AT*>(cval_v);
+  ctx->stats.split_rows = 0;
   int64_t off[kNumcBins + 1] = {0};
   for (int b = 0; b < kNumcBins; ++b) off[b + 1] = off[b] + c.numc_count[b];
   const int order[] = {kNB_Dense, kNB_E8K, kNB_H4K, kNB_E6K, kNB_E5K, kNB_E4K, kNB_E3K, kNB_H1K,
@@ -948,12 +1007,24 @@ cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* 
       case kNB_H4K:
         k_numc_hash<512, 13, VIn><<<(unsigned)n, 512, smem_numc_hash<512, 13, VIn>(), s>>>(rows, A, B, crp, ccol, cval, ctx->d_status);
         break;
-      case kNB_Dense:
+      case kNB_Dense: {
         if (!c.b_sorted && c.ncol > kRankCols)
           return set_err(ctx, CAS_ERR_BAD_INPUT, "heavy rows over more than %d columns need B rows sorted by column", kRankCols);
-        k_numc_dense<512, VIn><<<(unsigned)n, 512, smem_numc_dense<512, VIn>(), s>>>(
-            rows, A, B, c.ncol, c.b_sorted ? 1 : 0, crp, ccol, cval, c.dbits, c.dslot, ctx->d_status);
+        // the rows of at least kSplitProducts products (log2 size classes 18 and up) lead the
+        // bin's heaviest-first order; they are split across blocks when their scratch fits
+        int64_t n_split = 0;
+        for (int k = 0; k <= kHeavyClasses - 1 - 18; ++k) n_split += (int64_t)ctx->h_counts[kSlotHeavy + k];
+        n_split = std::min(n_split, n);
+        const int64_t max_slices = (c.ncol + kRankCols - 1) / kRankCols;
+        n_split = std::min<int64_t>(n_split, kSplitScratch / (max_slices * (kRankCols / 8)));
+        if (!ctx->heavy_split) n_split = 0;
+        ctx->stats.split_rows = n_split;
+        if (n_split > 0) CAS_TRY(launch_heavy_split<VIn>(ctx, c, rows, n_split, crp, ccol, cval, s));
+        if (n > n_split)
+          k_numc_dense<512, VIn><<<(unsigned)(n - n_split), 512, smem_numc_dense<512, VIn>(), s>>>(
+              rows + n_split, A, B, c.ncol, c.b_sorted ? 1 : 0, crp, ccol, cval, c.dbits, c.dslot, ctx->d_status);
         break;
+      }
     }
     CAS_TRY(check_launch(ctx, "numeric bin"));
     if (ctx->profile) CAS_CUDA(ctx, cudaEventRecord(ctx->ev_numc[1][b], s));
@@ -1279,7 +1350,7 @@ cas_status cas_set_tuning(cas_ctx* ctx, const cas_tuning* t) {
   if (!ctx || !t) return CAS_ERR_BAD_INPUT;
   if (!(t->acc_thres >= 0.0) || t->fused_min_products < 32 || t->fused_min_products >= (int)cas::kFusedHi ||
       t->esc_max_products < 32 || t->esc_max_products > 8192 || t->hash_max_nnz < 0 || t->hash_max_nnz > 4096 ||
-      t->esc_form < 0 || t->esc_form > 2)
+      t->esc_form < 0 || t->esc_form > 2 || (t->heavy_split != 0 && t->heavy_split != 1))
     return set_err(ctx, CAS_ERR_BAD_INPUT, "tuning out of range");
   ctx->acc_thres = t->acc_thres;
   ctx->fuse = t->fusion != 0;
@@ -1287,6 +1358,7 @@ cas_status cas_set_tuning(cas_ctx* ctx, const cas_tuning* t) {
   ctx->esc_max = t->esc_max_products;
   ctx->hash_max = t->hash_max_nnz;
   ctx->esc_form = t->esc_form;
+  ctx->heavy_split = t->heavy_split != 0;
   return CAS_OK;
 }
 
@@ -1298,6 +1370,7 @@ cas_status cas_get_tuning(const cas_ctx* ctx, cas_tuning* t) {
   t->esc_max_products = ctx->esc_max;
   t->hash_max_nnz = ctx->hash_max;
   t->esc_form = ctx->esc_form;
+  t->heavy_split = ctx->heavy_split ? 1 : 0;
   return CAS_OK;
 }
 

@@ -216,9 +216,8 @@ struct alignas(16) Stage {
 };
 
 template <int BLOCK, bool NEED_VAL, typename VIn, typename F>
-__device__ __forceinline__ int64_t expand_row(const Csr& A, const Csr& B, int64_t r, Stage<VIn>& sg,
-                                              bool ranged, int32_t c0, int32_t c1, F&& f) {
-  const int64_t as = A.rp[r], ae = A.rp[r + 1];
+__device__ __forceinline__ int64_t expand_entries(const Csr& A, const Csr& B, int64_t as, int64_t ae, Stage<VIn>& sg,
+                                                  bool ranged, int32_t c0, int32_t c1, F&& f) {
   const VIn* __restrict__ aval = static_cast<const VIn*>(A.val);
   const VIn* __restrict__ bval = static_cast<const VIn*>(B.val);
   constexpr int ACH = BLOCK < kAChunk ? BLOCK : kAChunk;  // one staged A entry per thread
@@ -300,6 +299,13 @@ __device__ __forceinline__ int64_t expand_row(const Csr& A, const Csr& B, int64_
     __syncthreads();
   }
   return pbase;
+}
+
+// The products of row r (its A entries [A.rp[r], A.rp[r + 1])).
+template <int BLOCK, bool NEED_VAL, typename VIn, typename F>
+__device__ __forceinline__ int64_t expand_row(const Csr& A, const Csr& B, int64_t r, Stage<VIn>& sg,
+                                              bool ranged, int32_t c0, int32_t c1, F&& f) {
+  return expand_entries<BLOCK, NEED_VAL, VIn>(A, B, A.rp[r], A.rp[r + 1], sg, ranged, c0, c1, f);
 }
 
 // ================================================================ SYMBOLIC
@@ -2056,6 +2062,242 @@ k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int
     __syncthreads();
   }
   if (threadIdx.x == 0 && written != nz) dev_report(st, written > nz ? kDevRowOverflow : kDevRowUnderflow, 13, r);
+}
+
+// ---- the heaviest rows over several blocks ----------------------------------
+// A dense row with kSplitProducts products or more is split across blocks
+// (the heavy-row regime the reference enters when the largest row's products
+// pass SMTACT_*_THRES, src/ams/ams_utils.c:1538-1550, there by using every
+// socket's cores).  k_dense_setup, one block per row, builds each column
+// slice's bitmap (or takes the one the symbolic kernel kept), writes C's
+// columns and zeroes its values as k_numc_dense does, and records for the
+// parts: the bitmaps, the entries of C before each slice, the row's product
+// prefix over its A entries and its part count.  k_dense_acc, a grid of
+// persistent blocks, then takes parts (row, q) in ticket order, heaviest row
+// first: part q of K takes the row's A entries whose products start in
+// [q P / K, (q + 1) P / K), and for each slice loads the bitmap, ranks its
+// words and adds its products into C by global atomics.  Because parts are
+// taken row by row, only a few rows are being added into at any time, so
+// their value ranges stay in L2, where the atomics resolve; a single block
+// per row (k_numc_dense) keeps hundreds of rows of megabytes each open at
+// once, and their atomics miss L2.
+constexpr int64_t kSplitProducts = int64_t(1) << 18;
+constexpr int64_t kPartProducts = int64_t(1) << 17;
+
+struct HeavyPlan {
+  const int32_t* rows;      // the split rows, heaviest first
+  int64_t n;                // their count
+  int max_slices;           // column slices a row can span: ceil(columns / kRankCols)
+  uint32_t* bits;           // n * max_slices bitmaps of kRankCols bits
+  int64_t* slice_base;      // n * max_slices: entries of the row's C before each slice
+  int64_t* lo;              // n: the row's first column
+  int64_t* hi;              // n: one past the row's last column
+  int32_t* nslices;         // n: slices the row spans
+  int64_t* products;        // n: the row's products
+  int64_t* nparts;          // n: parts of each row
+  int64_t* parts;           // n + 1: the first part of each row (the scan of nparts), then the total
+  int64_t* apre;            // per A entry of a split row (at its position in A): products of the
+                            // row's earlier entries
+  unsigned long long* ticket;
+};
+
+// Word ranks of a slice bitmap in shared memory: for each word the set bits
+// of the words before it in its group of 8 (wrank) and the set bits before
+// the group (gbase); returns the slice's set bits.
+template <int BLOCK>
+__device__ __forceinline__ long long slice_ranks(const uint32_t* __restrict__ bm, int nw, uint32_t* __restrict__ gbase,
+                                                 uint16_t* __restrict__ wrank, long long* tmp) {
+  const int ng = (nw + 7) >> 3;
+  long long run = 0;
+  for (int g0 = 0; g0 < ng; g0 += BLOCK) {
+    const int g = g0 + threadIdx.x;
+    int cnt = 0;
+    if (g < ng) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int w = g * 8 + k;
+        wrank[w] = (uint16_t)cnt;
+        cnt += w < nw ? __popc(bm[w]) : 0;
+      }
+    }
+    long long tot;
+    const long long ex = block_exclusive_sum<BLOCK, long long>((long long)cnt, tmp, tot);
+    if (g < ng) gbase[g] = (uint32_t)(run + ex);
+    run += tot;
+  }
+  __syncthreads();
+  return run;
+}
+
+// Exclusive scan of n counts into out[0..n], out[n] the total, by one block
+// (the split rows are at most a few thousand).
+__global__ void k_scan_one_block(const int64_t* __restrict__ in, int64_t n, int64_t* __restrict__ out) {
+  __shared__ long long tmp[33];
+  long long run = 0;
+  for (int64_t i0 = 0; i0 < n; i0 += 1024) {
+    const int64_t i = i0 + threadIdx.x;
+    const long long v = i < n ? in[i] : 0;
+    long long tot;
+    const long long ex = block_exclusive_sum<1024, long long>(v, tmp, tot);
+    if (i < n) out[i] = run + ex;
+    run += tot;
+  }
+  if (threadIdx.x == 0) out[n] = run;
+}
+
+template <int BLOCK, typename VIn>
+__global__ void __launch_bounds__(BLOCK)
+k_dense_setup(HeavyPlan hp, Csr A, Csr B, int64_t c_ncol, int32_t b_sorted, const int64_t* __restrict__ crp,
+              int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval, const uint32_t* __restrict__ saved,
+              const int32_t* __restrict__ saved_slot, DevStatus* st) {
+  using AT = typename Acc<VIn>::T;
+  constexpr int NWORD = kRankCols / 32;
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint32_t* bm = reinterpret_cast<uint32_t*>(smem);
+  uint32_t* gbase = bm + NWORD;
+  uint16_t* wrank = reinterpret_cast<uint16_t*>(gbase + NWORD / 8);
+  Stage<VIn>& sg = *reinterpret_cast<Stage<VIn>*>(reinterpret_cast<uint8_t*>(wrank + NWORD));
+  const int64_t i = blockIdx.x;
+  const int64_t r = hp.rows[i];
+  const int64_t c0r = crp[r], nz = crp[r + 1] - c0r;
+  const int64_t as = A.rp[r], ae = A.rp[r + 1];
+  // the row's product prefix over its A entries, and its part count
+  long long run = 0;
+  for (int64_t a0 = as; a0 < ae; a0 += BLOCK) {
+    long long len = 0;
+    if (a0 + threadIdx.x < ae) {
+      const int32_t k = A.col[a0 + threadIdx.x];
+      len = B.rp[k + 1] - B.rp[k];
+    }
+    long long tot;
+    const long long ex = block_exclusive_sum<BLOCK, long long>(len, sg.tmp, tot);
+    if (a0 + threadIdx.x < ae) hp.apre[a0 + threadIdx.x] = run + ex;
+    run += tot;
+  }
+  int64_t lo, hi;
+  row_col_range<BLOCK>(A, B, r, b_sorted != 0, c_ncol, lo, hi);
+  const int ns = hi > lo ? (int)((hi - lo + kRankCols - 1) / kRankCols) : 0;
+  if (threadIdx.x == 0) {
+    hp.products[i] = run;
+    hp.nparts[i] = ns > 0 ? (run + kPartProducts - 1) / kPartProducts : 0;
+    hp.lo[i] = lo;
+    hp.hi[i] = hi;
+    hp.nslices[i] = ns;
+    if (ns > hp.max_slices) dev_report(st, kDevCapacity, 14, r);
+  }
+  const bool multi = ns > 1;
+  int64_t written = 0;
+  for (int sl = 0; sl < ns && sl < hp.max_slices; ++sl) {
+    const int64_t s0 = lo + (int64_t)sl * kRankCols;
+    const int64_t s1 = hi < s0 + kRankCols ? hi : s0 + kRankCols;
+    const int nw = (int)((s1 - s0 + 31) >> 5);
+    const int32_t slot = (!multi && saved_slot) ? saved_slot[r] : -1;
+    if (slot >= 0) {
+      const uint32_t* src = saved + (size_t)slot * NWORD;
+      for (int w = threadIdx.x; w < nw; w += BLOCK) bm[w] = src[w];
+      __syncthreads();
+    } else {
+      for (int w = threadIdx.x; w < nw; w += BLOCK) bm[w] = 0u;
+      __syncthreads();
+      expand_row<BLOCK, false, VIn>(A, B, r, sg, multi, (int32_t)s0, (int32_t)s1, [&](int32_t key, VIn, VIn, int64_t) {
+        const int64_t idx = (int64_t)key - s0;
+        if (idx >= 0 && idx < kRankCols) atomicOr(&bm[idx >> 5], 1u << (idx & 31));
+      });
+      __syncthreads();
+    }
+    uint32_t* dst = hp.bits + ((size_t)i * hp.max_slices + sl) * NWORD;
+    for (int w = threadIdx.x; w < nw; w += BLOCK) dst[w] = bm[w];
+    if (threadIdx.x == 0) hp.slice_base[(size_t)i * hp.max_slices + sl] = written;
+    const long long cnt = slice_ranks<BLOCK>(bm, nw, gbase, wrank, sg.tmp);
+    const int64_t base = c0r + written;
+    const int64_t room = nz - written;
+    for (int w = threadIdx.x; w < nw; w += BLOCK) {
+      uint32_t word = bm[w];
+      int64_t pos = (int64_t)gbase[w >> 3] + wrank[w];
+      while (word) {
+        const int b = __ffs(word) - 1;
+        word &= word - 1;
+        if (pos < room) {
+          ccol[base + pos] = (int32_t)(s0 + w * 32 + b);
+          cval[base + pos] = AT(0);
+        }
+        ++pos;
+      }
+    }
+    written += cnt;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && written != nz) dev_report(st, written > nz ? kDevRowOverflow : kDevRowUnderflow, 14, r);
+}
+
+template <int BLOCK, typename VIn>
+__global__ void __launch_bounds__(BLOCK)
+k_dense_acc(HeavyPlan hp, Csr A, Csr B, const int64_t* __restrict__ crp, typename Acc<VIn>::T* __restrict__ cval,
+            DevStatus* st) {
+  constexpr int NWORD = kRankCols / 32;
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint32_t* bm = reinterpret_cast<uint32_t*>(smem);
+  uint32_t* gbase = bm + NWORD;
+  uint16_t* wrank = reinterpret_cast<uint16_t*>(gbase + NWORD / 8);
+  Stage<VIn>& sg = *reinterpret_cast<Stage<VIn>*>(reinterpret_cast<uint8_t*>(wrank + NWORD));
+  __shared__ long long s_t, s_i;
+  const int64_t total = hp.parts[hp.n];
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const long long t = (long long)atomicAdd(hp.ticket, 1ull);
+      int64_t lo = 0, hi = hp.n;  // the row i with parts[i] <= t < parts[i + 1]
+      while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (hp.parts[mid] <= t) lo = mid; else hi = mid;
+      }
+      s_t = t;
+      s_i = lo;
+    }
+    __syncthreads();
+    const int64_t t = s_t, i = s_i;
+    __syncthreads();
+    if (t >= total) break;
+    const int64_t r = hp.rows[i];
+    const int64_t K = hp.parts[i + 1] - hp.parts[i], q = t - hp.parts[i];
+    const int64_t P = hp.products[i];
+    const int64_t as = A.rp[r], ae = A.rp[r + 1];
+    // A entries whose products start in [q P / K, (q + 1) P / K)
+    auto first_at = [&](int64_t target) -> int64_t {  // first entry whose prefix is >= target
+      int64_t l = as, h = ae;
+      while (l < h) {
+        const int64_t mid = (l + h) >> 1;
+        if (hp.apre[mid] < target) l = mid + 1; else h = mid;
+      }
+      return l;
+    };
+    const int64_t a0 = q == 0 ? as : first_at(P * q / K);
+    const int64_t a1 = q + 1 == K ? ae : first_at(P * (q + 1) / K);
+    const int ns = hp.nslices[i];
+    const int64_t lo = hp.lo[i], hi = hp.hi[i];
+    const int64_t c0r = crp[r];
+    for (int sl = 0; sl < ns && a1 > a0; ++sl) {
+      const int64_t s0 = lo + (int64_t)sl * kRankCols;
+      const int64_t s1 = hi < s0 + kRankCols ? hi : s0 + kRankCols;
+      const int nw = (int)((s1 - s0 + 31) >> 5);
+      const uint32_t* src = hp.bits + ((size_t)i * hp.max_slices + sl) * NWORD;
+      const int64_t sb = hp.slice_base[(size_t)i * hp.max_slices + sl];
+      for (int w = threadIdx.x; w < nw; w += BLOCK) bm[w] = src[w];
+      __syncthreads();
+      slice_ranks<BLOCK>(bm, nw, gbase, wrank, sg.tmp);
+      const int64_t base = c0r + sb;
+      expand_entries<BLOCK, true, VIn>(A, B, a0, a1, sg, ns > 1, (int32_t)s0, (int32_t)s1,
+                                       [&](int32_t key, VIn av, VIn bv, int64_t) {
+        const int64_t idx = (int64_t)key - s0;
+        if (idx < 0 || idx >= s1 - s0) return;
+        const int w = (int)(idx >> 5);
+        const uint32_t m = bm[w];
+        if (!((m >> (idx & 31)) & 1u)) return;  // cannot happen for a consistent bitmap
+        const int64_t pos = (int64_t)gbase[w >> 3] + wrank[w] + __popc(m & ((1u << (idx & 31)) - 1u));
+        Acc<VIn>::atomic_add(&cval[base + pos], Acc<VIn>::mul(av, bv));
+      });
+      __syncthreads();
+    }
+  }
 }
 
 }  // namespace cas

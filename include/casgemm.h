@@ -108,6 +108,8 @@ typedef struct {
 	/* of d2h_bytes, those copied by DMA straight into host blocks the
 	 * context has registered (blocks it kept from earlier outputs) */
 	double d2h_direct_bytes;
+	/* dense rows split across thread blocks (cas_tuning.heavy_split) */
+	int64_t split_rows;
 } cas_stats;
 
 typedef struct cas_ctx cas_ctx;
@@ -152,6 +154,9 @@ typedef struct {
 	                                32 products or more, a warp per B row in the value pass (rows of
 	                                up to 6144 products; larger ones take form 1); 0 keeps column and
 	                                value, 3 rows per SM */
+	int32_t heavy_split;         /* 1: dense rows of 2^18 products or more are split across thread blocks
+	                                by A-entry ranges, heaviest row first, adding into C by atomics that
+	                                stay in L2 [1]; 0: one block per dense row */
 } cas_tuning;
 cas_status cas_set_tuning(cas_ctx *ctx, const cas_tuning *t);
 cas_status cas_get_tuning(const cas_ctx *ctx, cas_tuning *t);
