@@ -450,6 +450,8 @@ def main():
                     help="pick the row routing with casgemm.Autotuner (cached in CACHE.json) before timing")
     ap.add_argument("--esc-form", type=int, default=None, choices=[0, 1, 2],
                     help="bucketed ESC kernel form (cas_tuning.esc_form); default: the library's")
+    ap.add_argument("--heavy-split", type=int, default=None, choices=[0, 1],
+                    help="split the heaviest dense rows across blocks (cas_tuning.heavy_split); default: the library's")
     ap.add_argument("--assemble", action="store_true",
                     help="N > 1: assemble C's row shards on rank 0 after the timed steps (reported, not timed)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -500,6 +502,8 @@ def main():
     tuning = None
     if args.esc_form is not None:
         ctx.set_tuning(esc_form=args.esc_form)
+    if args.heavy_split is not None:
+        ctx.set_tuning(heavy_split=args.heavy_split)
     if args.tune:
         tuner = casgemm.Autotuner(ctx, args.tune)
         key = casgemm.Autotuner.key(As, B)
