@@ -1695,21 +1695,81 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   // warp), then the warp's buckets of 9..kBucketLimit pairs one at a time;
   // a bucket of more pairs over at most kHugeWidth columns (hub columns) is
   // left to the whole block
-  for (int g = warp; g < NG; g += NW) {
-    const int b = g * 32 + lane;
-    const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
-    if (e - s > kBucketLimit) s_huge = b;
-    const int small = (e - s <= 8) ? e - s : 0;
-    const int mx = __reduce_max_sync(kFull, small);
-    if (small > 1) {
-      const uint32_t kbase = lo + ((uint32_t)b << shift);
-      if (mx <= 4) sort_perm_small<4>(skey, sidx, s, e, kbase);
-      else if (mx <= 6) sort_perm_small<6>(skey, sidx, s, e, kbase);
-      else sort_perm_small<8>(skey, sidx, s, e, kbase);
+  if constexpr (REGK) {
+    // the warp's buckets of 2, 3-4 and 5-8 pairs gather in three queues
+    // (in place_of, which the place pass fills later) and are sorted 32 at a
+    // time, each by the network of its size, so a lane never runs a network
+    // padded to the largest bucket of its group
+    uint16_t* wq = place_of + warp * (3 * 64);
+    int qn[3] = {0, 0, 0};
+    auto run_queue = [&](int k, int cnt) {
+      if (lane < cnt) {
+        const int b = wq[k * 64 + lane];
+        const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
+        if (k == 0) {
+          const uint32_t k0 = skey[s], k1 = skey[s + 1];
+          if (k1 < k0) {
+            skey[s] = k1;
+            skey[s + 1] = k0;
+            const uint16_t i0 = sidx[s];
+            sidx[s] = sidx[s + 1];
+            sidx[s + 1] = i0;
+          }
+        } else {
+          const uint32_t kbase = lo + ((uint32_t)b << shift);
+          if (k == 1) sort_perm_small<4>(skey, sidx, s, e, kbase);
+          else sort_perm_small<8>(skey, sidx, s, e, kbase);
+        }
+      }
+    };
+    for (int g = warp; g < NG; g += NW) {
+      const int b = g * 32 + lane;
+      const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
+      const int nb = e - s;
+      if (nb > kBucketLimit) s_huge = b;
+      const int cls = nb == 2 ? 0 : (nb == 3 || nb == 4) ? 1 : (nb >= 5 && nb <= 8) ? 2 : -1;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const unsigned m = __ballot_sync(kFull, cls == k);
+        if (cls == k) wq[k * 64 + qn[k] + __popc(m & lanemask_lt())] = (uint16_t)b;
+        qn[k] += __popc(m);
+        if (qn[k] >= 32) {
+          __syncwarp();
+          run_queue(k, 32);
+          const int rest = qn[k] - 32;
+          const uint16_t mv = lane < rest ? wq[k * 64 + 32 + lane] : uint16_t(0);
+          __syncwarp();
+          if (lane < rest) wq[k * 64 + lane] = mv;
+          __syncwarp();
+          qn[k] = rest;
+        }
+      }
+      for (unsigned bigm = __ballot_sync(kFull, nb > 8 && nb <= kBucketLimit); bigm; bigm &= bigm - 1) {
+        const int l = __ffs(bigm) - 1;
+        warp_sort_perm(skey, sidx, __shfl_sync(kFull, s, l), __shfl_sync(kFull, e, l));
+      }
     }
-    for (unsigned bigm = __ballot_sync(kFull, e - s > 8 && e - s <= kBucketLimit); bigm; bigm &= bigm - 1) {
-      const int l = __ffs(bigm) - 1;
-      warp_sort_perm(skey, sidx, __shfl_sync(kFull, s, l), __shfl_sync(kFull, e, l));
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      if (qn[k] > 0) run_queue(k, qn[k]);
+  } else {
+    for (int g = warp; g < NG; g += NW) {
+      const int b = g * 32 + lane;
+      const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
+      if (e - s > kBucketLimit) s_huge = b;
+      const int small = (e - s <= 8) ? e - s : 0;
+      const int mx = __reduce_max_sync(kFull, small);
+      if (small > 1) {
+        const uint32_t kbase = lo + ((uint32_t)b << shift);
+        if (mx <= 4) sort_perm_small<4>(skey, sidx, s, e, kbase);
+        else if (mx <= 6) sort_perm_small<6>(skey, sidx, s, e, kbase);
+        else sort_perm_small<8>(skey, sidx, s, e, kbase);
+      }
+      for (unsigned bigm = __ballot_sync(kFull, e - s > 8 && e - s <= kBucketLimit); bigm; bigm &= bigm - 1) {
+        const int l = __ffs(bigm) - 1;
+        warp_sort_perm(skey, sidx, __shfl_sync(kFull, s, l), __shfl_sync(kFull, e, l));
+      }
     }
   }
   __syncthreads();
