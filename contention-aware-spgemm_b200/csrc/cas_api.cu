@@ -70,7 +70,7 @@ struct cas_ctx {
   bool fuse = true;                        // fused ESC rows (no symbolic pass) in cas_spgemm
   int fused_lo = (int)cas::kFusedLo;       // fused rows: more products than this (up to kFusedHi)
   bool heavy_split = true;                 // dense rows of 2^18 products or more split across blocks
-  int esc_form = 1;                        // bucketed ESC of rows over 4096 products (fused rows included):
+  int esc_form = 2;                        // bucketed ESC of rows over 4096 products (fused rows included):
                                            // 1 index form (k_numc_esc_idx), 0 k_numc_esc_msd, 2 the index
                                            // form with the keys in registers between its two key passes
   int esc_max = 8192;                      // ESC rows: at most this many products
@@ -252,6 +252,7 @@ cas_status setup_kernels(cas_ctx* ctx) {
   CAS_SYMB_SHAPES(CAS_SETUP_SYMB)
 #undef CAS_SETUP_SYMB
   CAS_TRY(allow_smem(ctx, k_symb_dense<512>, smem_symb_dense<512>()));
+  CAS_TRY(allow_smem(ctx, k_heavy_bits<512>, smem_symb_dense<512>()));
   CAS_TRY(setup_numc_kernels<double>(ctx));
   CAS_TRY(setup_numc_kernels<int32_t>(ctx));
   return CAS_OK;
@@ -625,6 +626,11 @@ struct Call {
   // bitmaps of heavy rows kept by the symbolic kernel for the numeric one
   uint32_t* dbits = nullptr;
   int32_t* dslot = nullptr;
+  // the symbolic phase's split rows: their slice bitmaps, and each row's slot
+  // in them (-1 for other rows); kept for the numeric setup of split rows
+  uint32_t* hbits = nullptr;
+  int32_t* hslot = nullptr;
+  std::vector<void*> heavy_tmp;  // the rest of the symbolic split's scratch
 };
 
 cas_status fork(cas_ctx* ctx) {
@@ -662,6 +668,10 @@ cas_status scratch_free(cas_ctx* ctx, Call& c) {
   c.fstatus = nullptr;
   c.dbits = nullptr;
   c.dslot = nullptr;
+  for (void* p : c.heavy_tmp) CAS_CUDA(ctx, cudaFreeAsync(p, ctx->stream));
+  c.heavy_tmp.clear();
+  c.hbits = nullptr;
+  c.hslot = nullptr;
   return CAS_OK;
 }
 
@@ -784,6 +794,74 @@ cas_status launch_fused(cas_ctx* ctx, Call& c, const int64_t* known, int32_t* cc
   return CAS_OK;
 }
 
+constexpr int64_t kSplitScratch = int64_t(8) << 30;  // at most 8 GiB of slice bitmaps per phase
+
+// The symbolic phase's split rows (see k_heavy_plan in cas_kernels.cu): the
+// dense symbolic rows of at least kSplitProducts products, up to the scratch
+// cap, get their slice bitmaps built by parts over many blocks and their
+// counts from those bitmaps; the rest stay in `rows`, and their number in n.
+cas_status symb_split_heavy(cas_ctx* ctx, Call& c, int32_t*& rows, int64_t& n, int64_t* row_nz, cudaStream_t s) {
+  using namespace cas;
+  const int64_t max_slices = (c.ncol + kRankCols - 1) / kRankCols;
+  const int64_t cap = kSplitScratch / (max_slices * (kRankCols / 8));
+  auto alloc = [&](void** p, size_t bytes) -> cas_status {
+    cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, s);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(ctx, e == cudaErrorMemoryAllocation ? CAS_ERR_OOM : CAS_ERR_CUDA,
+                     "device allocation of %zu bytes for the split rows failed", bytes);
+    }
+    c.heavy_tmp.push_back(*p);
+    return CAS_OK;
+  };
+  int32_t *heavy = nullptr, *light = nullptr;
+  unsigned long long* counts = nullptr;
+  CAS_TRY(alloc((void**)&c.hslot, sizeof(int32_t) * (size_t)(c.m + 1)));
+  CAS_TRY(alloc((void**)&heavy, sizeof(int32_t) * (size_t)n));
+  CAS_TRY(alloc((void**)&light, sizeof(int32_t) * (size_t)n));
+  CAS_TRY(alloc((void**)&counts, 2 * sizeof(unsigned long long)));
+  CAS_CUDA(ctx, cudaMemsetAsync(c.hslot, 0xFF, sizeof(int32_t) * (size_t)(c.m + 1), s));
+  CAS_CUDA(ctx, cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), s));
+  k_split_dense_rows<<<grid_for(n, 256, ctx->sm_count * 4), 256, 0, s>>>(rows, n, c.row_flp, cap, heavy, light, counts,
+                                                                          c.hslot);
+  CAS_TRY(check_launch(ctx, "k_split_dense_rows"));
+  unsigned long long h[2] = {0, 0};
+  CAS_CUDA(ctx, cudaMemcpyAsync(h, counts, sizeof(h), cudaMemcpyDeviceToHost, s));
+  CAS_CUDA(ctx, cudaStreamSynchronize(s));
+  const int64_t nh = std::min<int64_t>((int64_t)h[0], cap);
+  rows = light;
+  n = (int64_t)h[1];
+  if (nh == 0) return CAS_OK;
+  HeavyPlan hp{};
+  hp.rows = heavy;
+  hp.n = nh;
+  hp.max_slices = (int)max_slices;
+  CAS_TRY(alloc((void**)&hp.bits, (size_t)nh * max_slices * (kRankCols / 8)));
+  CAS_TRY(alloc((void**)&hp.slice_base, sizeof(int64_t) * (size_t)nh * max_slices));
+  CAS_TRY(alloc((void**)&hp.lo, sizeof(int64_t) * (size_t)nh));
+  CAS_TRY(alloc((void**)&hp.hi, sizeof(int64_t) * (size_t)nh));
+  CAS_TRY(alloc((void**)&hp.nslices, sizeof(int32_t) * (size_t)nh));
+  CAS_TRY(alloc((void**)&hp.products, sizeof(int64_t) * (size_t)nh));
+  CAS_TRY(alloc((void**)&hp.nparts, sizeof(int64_t) * (size_t)nh));
+  CAS_TRY(alloc((void**)&hp.parts, sizeof(int64_t) * (size_t)(nh + 1)));
+  CAS_TRY(alloc((void**)&hp.apre, sizeof(int64_t) * (size_t)(c.A.nnz > 0 ? c.A.nnz : 1)));
+  CAS_TRY(alloc((void**)&hp.ticket, sizeof(unsigned long long)));
+  c.hbits = hp.bits;
+  CAS_CUDA(ctx, cudaMemsetAsync(hp.ticket, 0, sizeof(unsigned long long), s));
+  k_heavy_plan<512><<<(unsigned)nh, 512, 0, s>>>(hp, c.A.csr, c.B.csr, c.ncol, c.b_sorted ? 1 : 0, ctx->d_status);
+  CAS_TRY(check_launch(ctx, "k_heavy_plan"));
+  k_scan_one_block<<<1, 1024, 0, s>>>(hp.nparts, nh, hp.parts);
+  CAS_TRY(check_launch(ctx, "k_scan_one_block"));
+  int per_sm = 0;
+  CAS_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_heavy_bits<512>, 512, smem_symb_dense<512>()));
+  k_heavy_bits<512><<<std::max(1, per_sm) * ctx->sm_count, 512, smem_symb_dense<512>(), s>>>(hp, c.A.csr, c.B.csr,
+                                                                                             ctx->d_status);
+  CAS_TRY(check_launch(ctx, "k_heavy_bits"));
+  k_heavy_count<512><<<(unsigned)nh, 512, 0, s>>>(hp, row_nz);
+  CAS_TRY(check_launch(ctx, "k_heavy_count"));
+  return CAS_OK;
+}
+
 // ------------------------------------------------------------------ SYMB
 cas_status launch_symb_bins(cas_ctx* ctx, Call& c, int64_t* row_nz) {
   using namespace cas;
@@ -811,20 +889,29 @@ cas_status launch_symb_bins(cas_ctx* ctx, Call& c, int64_t* row_nz) {
         break;
       CAS_SYMB_SHAPES(CAS_SYMB_CASE)
 #undef CAS_SYMB_CASE
-      case kSB_Dense:
+      case kSB_Dense: {
         if (!c.b_sorted && c.ncol > kDenseChunkBits)
           return set_err(ctx, CAS_ERR_BAD_INPUT, "heavy rows over more than %d columns need B rows sorted by column", kDenseChunkBits);
-        if ((double)n * (kRankCols / 8) <= kSavedBitmapBytes) {  // bitmaps kept for the numeric kernel
-          CAS_TRY(dev_alloc(ctx, (void**)&c.dbits, (size_t)n * (kRankCols / 8)));
+        int32_t* drows = const_cast<int32_t*>(rows);
+        int64_t nd = n;
+        if (ctx->heavy_split) {
+          CAS_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
+          CAS_CUDA(ctx, cudaStreamWaitEvent(s, ctx->ev_fork, 0));
+          CAS_TRY(symb_split_heavy(ctx, c, drows, nd, row_nz, s));
+        }
+        if (nd == 0) break;
+        if ((double)nd * (kRankCols / 8) <= kSavedBitmapBytes) {  // bitmaps kept for the numeric kernel
+          CAS_TRY(dev_alloc(ctx, (void**)&c.dbits, (size_t)nd * (kRankCols / 8)));
           CAS_TRY(dev_alloc(ctx, (void**)&c.dslot, sizeof(int32_t) * (c.m + 1)));
           CAS_CUDA(ctx, cudaMemsetAsync(c.dslot, 0xFF, sizeof(int32_t) * (c.m + 1), ctx->stream));
           CAS_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
           CAS_CUDA(ctx, cudaStreamWaitEvent(s, ctx->ev_fork, 0));
         }
-        k_symb_dense<512><<<(unsigned)n, 512, smem_symb_dense<512>(), s>>>(rows, c.A.csr, c.B.csr, c.ncol,
-                                                                            c.b_sorted ? 1 : 0, row_nz, c.dbits,
-                                                                            c.dslot, ctx->d_status);
+        k_symb_dense<512><<<(unsigned)nd, 512, smem_symb_dense<512>(), s>>>(drows, c.A.csr, c.B.csr, c.ncol,
+                                                                             c.b_sorted ? 1 : 0, row_nz, c.dbits,
+                                                                             c.dslot, ctx->d_status);
         break;
+      }
     }
     CAS_TRY(check_launch(ctx, "symbolic bin"));
     if (ctx->profile) CAS_CUDA(ctx, cudaEventRecord(ctx->ev_symb[1][b], s));
@@ -912,7 +999,6 @@ void launch_esc_bin(int esc_form, int64_t n, cudaStream_t s, const int32_t* rows
 // k_dense_acc; see cas_kernels.cu), on stream s, with scratch allocated and
 // freed on s: the slice bitmaps (64 KiB per row and slice), the per-row
 // plan and the product prefix of every A entry.
-constexpr int64_t kSplitScratch = int64_t(8) << 30;  // at most 8 GiB of slice bitmaps
 
 template <typename VIn>
 cas_status launch_heavy_split(cas_ctx* ctx, Call& c, const int32_t* rows, int64_t n, const int64_t* crp, int32_t* ccol,
@@ -946,7 +1032,8 @@ cas_status launch_heavy_split(cas_ctx* ctx, Call& c, const int32_t* rows, int64_
     CAS_TRY(alloc((void**)&hp.ticket, sizeof(unsigned long long)));
     CAS_CUDA(ctx, cudaMemsetAsync(hp.ticket, 0, sizeof(unsigned long long), s));
     k_dense_setup<512, VIn><<<(unsigned)n, 512, smem_numc_dense<512, VIn>(), s>>>(
-        hp, c.A.csr, c.B.csr, c.ncol, c.b_sorted ? 1 : 0, crp, ccol, cval, c.dbits, c.dslot, ctx->d_status);
+        hp, c.A.csr, c.B.csr, c.ncol, c.b_sorted ? 1 : 0, crp, ccol, cval, c.dbits, c.dslot, c.hbits, c.hslot,
+        ctx->d_status);
     CAS_TRY(check_launch(ctx, "k_dense_setup"));
     k_scan_one_block<<<1, 1024, 0, s>>>(hp.nparts, n, hp.parts);
     CAS_TRY(check_launch(ctx, "k_scan_one_block"));

@@ -1695,81 +1695,21 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   // warp), then the warp's buckets of 9..kBucketLimit pairs one at a time;
   // a bucket of more pairs over at most kHugeWidth columns (hub columns) is
   // left to the whole block
-  if constexpr (REGK) {
-    // the warp's buckets of 2, 3-4 and 5-8 pairs gather in three queues
-    // (in place_of, which the place pass fills later) and are sorted 32 at a
-    // time, each by the network of its size, so a lane never runs a network
-    // padded to the largest bucket of its group
-    uint16_t* wq = place_of + warp * (3 * 64);
-    int qn[3] = {0, 0, 0};
-    auto run_queue = [&](int k, int cnt) {
-      if (lane < cnt) {
-        const int b = wq[k * 64 + lane];
-        const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
-        if (k == 0) {
-          const uint32_t k0 = skey[s], k1 = skey[s + 1];
-          if (k1 < k0) {
-            skey[s] = k1;
-            skey[s + 1] = k0;
-            const uint16_t i0 = sidx[s];
-            sidx[s] = sidx[s + 1];
-            sidx[s + 1] = i0;
-          }
-        } else {
-          const uint32_t kbase = lo + ((uint32_t)b << shift);
-          if (k == 1) sort_perm_small<4>(skey, sidx, s, e, kbase);
-          else sort_perm_small<8>(skey, sidx, s, e, kbase);
-        }
-      }
-    };
-    for (int g = warp; g < NG; g += NW) {
-      const int b = g * 32 + lane;
-      const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
-      const int nb = e - s;
-      if (nb > kBucketLimit) s_huge = b;
-      const int cls = nb == 2 ? 0 : (nb == 3 || nb == 4) ? 1 : (nb >= 5 && nb <= 8) ? 2 : -1;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const unsigned m = __ballot_sync(kFull, cls == k);
-        if (cls == k) wq[k * 64 + qn[k] + __popc(m & lanemask_lt())] = (uint16_t)b;
-        qn[k] += __popc(m);
-        if (qn[k] >= 32) {
-          __syncwarp();
-          run_queue(k, 32);
-          const int rest = qn[k] - 32;
-          const uint16_t mv = lane < rest ? wq[k * 64 + 32 + lane] : uint16_t(0);
-          __syncwarp();
-          if (lane < rest) wq[k * 64 + lane] = mv;
-          __syncwarp();
-          qn[k] = rest;
-        }
-      }
-      for (unsigned bigm = __ballot_sync(kFull, nb > 8 && nb <= kBucketLimit); bigm; bigm &= bigm - 1) {
-        const int l = __ffs(bigm) - 1;
-        warp_sort_perm(skey, sidx, __shfl_sync(kFull, s, l), __shfl_sync(kFull, e, l));
-      }
+  for (int g = warp; g < NG; g += NW) {
+    const int b = g * 32 + lane;
+    const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
+    if (e - s > kBucketLimit) s_huge = b;
+    const int small = (e - s <= 8) ? e - s : 0;
+    const int mx = __reduce_max_sync(kFull, small);
+    if (small > 1) {
+      const uint32_t kbase = lo + ((uint32_t)b << shift);
+      if (mx <= 4) sort_perm_small<4>(skey, sidx, s, e, kbase);
+      else if (mx <= 6) sort_perm_small<6>(skey, sidx, s, e, kbase);
+      else sort_perm_small<8>(skey, sidx, s, e, kbase);
     }
-    __syncwarp();
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-      if (qn[k] > 0) run_queue(k, qn[k]);
-  } else {
-    for (int g = warp; g < NG; g += NW) {
-      const int b = g * 32 + lane;
-      const int s = b ? (int)bucket_get(bcnt, b - 1) : 0, e = (int)bucket_get(bcnt, b);
-      if (e - s > kBucketLimit) s_huge = b;
-      const int small = (e - s <= 8) ? e - s : 0;
-      const int mx = __reduce_max_sync(kFull, small);
-      if (small > 1) {
-        const uint32_t kbase = lo + ((uint32_t)b << shift);
-        if (mx <= 4) sort_perm_small<4>(skey, sidx, s, e, kbase);
-        else if (mx <= 6) sort_perm_small<6>(skey, sidx, s, e, kbase);
-        else sort_perm_small<8>(skey, sidx, s, e, kbase);
-      }
-      for (unsigned bigm = __ballot_sync(kFull, e - s > 8 && e - s <= kBucketLimit); bigm; bigm &= bigm - 1) {
-        const int l = __ffs(bigm) - 1;
-        warp_sort_perm(skey, sidx, __shfl_sync(kFull, s, l), __shfl_sync(kFull, e, l));
-      }
+    for (unsigned bigm = __ballot_sync(kFull, e - s > 8 && e - s <= kBucketLimit); bigm; bigm &= bigm - 1) {
+      const int l = __ffs(bigm) - 1;
+      warp_sort_perm(skey, sidx, __shfl_sync(kFull, s, l), __shfl_sync(kFull, e, l));
     }
   }
   __syncthreads();
@@ -2209,7 +2149,8 @@ template <int BLOCK, typename VIn>
 __global__ void __launch_bounds__(BLOCK)
 k_dense_setup(HeavyPlan hp, Csr A, Csr B, int64_t c_ncol, int32_t b_sorted, const int64_t* __restrict__ crp,
               int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval, const uint32_t* __restrict__ saved,
-              const int32_t* __restrict__ saved_slot, DevStatus* st) {
+              const int32_t* __restrict__ saved_slot, const uint32_t* __restrict__ sym_bits,
+              const int32_t* __restrict__ sym_slot, DevStatus* st) {
   using AT = typename Acc<VIn>::T;
   constexpr int NWORD = kRankCols / 32;
   extern __shared__ __align__(16) uint8_t smem[];
@@ -2252,7 +2193,12 @@ k_dense_setup(HeavyPlan hp, Csr A, Csr B, int64_t c_ncol, int32_t b_sorted, cons
     const int64_t s1 = hi < s0 + kRankCols ? hi : s0 + kRankCols;
     const int nw = (int)((s1 - s0 + 31) >> 5);
     const int32_t slot = (!multi && saved_slot) ? saved_slot[r] : -1;
-    if (slot >= 0) {
+    const int32_t hslot = sym_slot ? sym_slot[r] : -1;  // the symbolic phase's split bitmaps
+    if (hslot >= 0) {
+      const uint32_t* src = sym_bits + ((size_t)hslot * hp.max_slices + sl) * NWORD;
+      for (int w = threadIdx.x; w < nw; w += BLOCK) bm[w] = src[w];
+      __syncthreads();
+    } else if (slot >= 0) {
       const uint32_t* src = saved + (size_t)slot * NWORD;
       for (int w = threadIdx.x; w < nw; w += BLOCK) bm[w] = src[w];
       __syncthreads();
@@ -2360,4 +2306,150 @@ k_dense_acc(HeavyPlan hp, Csr A, Csr B, const int64_t* __restrict__ crp, typenam
   }
 }
 
+// ---- symbolic bitmaps of the heaviest rows over several blocks ---------------
+// The same split for the symbolic phase: the dense symbolic rows of at least
+// kSplitProducts products are moved to their own list (k_split_dense_rows),
+// one block per row plans the parts and clears the row's slice bitmaps
+// (k_heavy_plan), persistent blocks take the parts in ticket order, build
+// the part's bitmap of each slice in shared memory and OR its nonzero words
+// into the row's bitmap in global memory (k_heavy_bits), and one block per
+// row counts the bits (k_heavy_count: the row's distinct columns, and the
+// entries before each slice).  The bitmaps stay for the numeric phase, whose
+// setup copies them instead of expanding the row's products again.
+__global__ void k_split_dense_rows(const int32_t* __restrict__ rows, int64_t n, const int64_t* __restrict__ row_flp,
+                                   int64_t cap, int32_t* __restrict__ heavy, int32_t* __restrict__ light,
+                                   unsigned long long* __restrict__ counts, int32_t* __restrict__ hslot) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t r = rows[i];
+    bool h = row_flp[r] >= kSplitProducts;
+    if (h) {
+      const unsigned long long j = atomicAdd(&counts[0], 1ull);
+      if ((int64_t)j < cap) {
+        heavy[j] = r;
+        hslot[r] = (int32_t)j;
+      } else {
+        h = false;
+      }
+    }
+    if (!h) light[atomicAdd(&counts[1], 1ull)] = r;
+  }
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_heavy_plan(HeavyPlan hp, Csr A, Csr B, int64_t c_ncol, int32_t b_sorted, DevStatus* st) {
+  __shared__ long long tmp[33];
+  const int64_t i = blockIdx.x;
+  const int64_t r = hp.rows[i];
+  const int64_t as = A.rp[r], ae = A.rp[r + 1];
+  long long run = 0;
+  for (int64_t a0 = as; a0 < ae; a0 += BLOCK) {
+    long long len = 0;
+    if (a0 + threadIdx.x < ae) {
+      const int32_t k = A.col[a0 + threadIdx.x];
+      len = B.rp[k + 1] - B.rp[k];
+    }
+    long long tot;
+    const long long ex = block_exclusive_sum<BLOCK, long long>(len, tmp, tot);
+    if (a0 + threadIdx.x < ae) hp.apre[a0 + threadIdx.x] = run + ex;
+    run += tot;
+  }
+  int64_t lo, hi;
+  row_col_range<BLOCK>(A, B, r, b_sorted != 0, c_ncol, lo, hi);
+  const int ns = hi > lo ? (int)((hi - lo + kRankCols - 1) / kRankCols) : 0;
+  if (threadIdx.x == 0) {
+    hp.products[i] = run;
+    hp.nparts[i] = ns > 0 ? (run + kPartProducts - 1) / kPartProducts : 0;
+    hp.lo[i] = lo;
+    hp.hi[i] = hi;
+    hp.nslices[i] = ns;
+    if (ns > hp.max_slices) dev_report(st, kDevCapacity, 15, r);
+  }
+  uint32_t* bits = hp.bits + (size_t)i * hp.max_slices * (kRankCols / 32);
+  const int64_t words = (int64_t)(ns < hp.max_slices ? ns : hp.max_slices) * (kRankCols / 32);
+  for (int64_t w = threadIdx.x; w < words; w += BLOCK) bits[w] = 0u;
+}
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_heavy_bits(HeavyPlan hp, Csr A, Csr B, DevStatus* st) {
+  constexpr int NWORD = kRankCols / 32;
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint32_t* bm = reinterpret_cast<uint32_t*>(smem);
+  Stage<double>& sg = *reinterpret_cast<Stage<double>*>(smem + NWORD * sizeof(uint32_t));
+  __shared__ long long s_t, s_i;
+  const int64_t total = hp.parts[hp.n];
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const long long t = (long long)atomicAdd(hp.ticket, 1ull);
+      int64_t lo = 0, hi = hp.n;
+      while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (hp.parts[mid] <= t) lo = mid; else hi = mid;
+      }
+      s_t = t;
+      s_i = lo;
+    }
+    __syncthreads();
+    const int64_t t = s_t, i = s_i;
+    __syncthreads();
+    if (t >= total) break;
+    const int64_t r = hp.rows[i];
+    const int64_t K = hp.parts[i + 1] - hp.parts[i], q = t - hp.parts[i];
+    const int64_t P = hp.products[i];
+    const int64_t as = A.rp[r], ae = A.rp[r + 1];
+    auto first_at = [&](int64_t target) -> int64_t {
+      int64_t l = as, h = ae;
+      while (l < h) {
+        const int64_t mid = (l + h) >> 1;
+        if (hp.apre[mid] < target) l = mid + 1; else h = mid;
+      }
+      return l;
+    };
+    const int64_t a0 = q == 0 ? as : first_at(P * q / K);
+    const int64_t a1 = q + 1 == K ? ae : first_at(P * (q + 1) / K);
+    const int ns = hp.nslices[i] < hp.max_slices ? hp.nslices[i] : hp.max_slices;
+    const int64_t lo = hp.lo[i], hi = hp.hi[i];
+    for (int sl = 0; sl < ns && a1 > a0; ++sl) {
+      const int64_t s0 = lo + (int64_t)sl * kRankCols;
+      const int64_t s1 = hi < s0 + kRankCols ? hi : s0 + kRankCols;
+      const int nw = (int)((s1 - s0 + 31) >> 5);
+      for (int w = threadIdx.x; w < nw; w += BLOCK) bm[w] = 0u;
+      __syncthreads();
+      expand_entries<BLOCK, false, double>(A, B, a0, a1, sg, ns > 1, (int32_t)s0, (int32_t)s1,
+                                           [&](int32_t key, double, double, int64_t) {
+        const int64_t idx = (int64_t)key - s0;
+        if (idx >= 0 && idx < s1 - s0) atomicOr(&bm[idx >> 5], 1u << (idx & 31));
+      });
+      __syncthreads();
+      uint32_t* g = hp.bits + ((size_t)i * hp.max_slices + sl) * NWORD;
+      for (int w = threadIdx.x; w < nw; w += BLOCK) {
+        const uint32_t v = bm[w];
+        if (v) atomicOr(&g[w], v);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_heavy_count(HeavyPlan hp, int64_t* __restrict__ row_nz) {
+  __shared__ long long tmp[33];
+  const int64_t i = blockIdx.x;
+  const int ns = hp.nslices[i] < hp.max_slices ? hp.nslices[i] : hp.max_slices;
+  const int64_t lo = hp.lo[i], hi = hp.hi[i];
+  long long run = 0;
+  for (int sl = 0; sl < ns; ++sl) {
+    const int64_t s0 = lo + (int64_t)sl * kRankCols;
+    const int64_t s1 = hi < s0 + kRankCols ? hi : s0 + kRankCols;
+    const int nw = (int)((s1 - s0 + 31) >> 5);
+    const uint32_t* g = hp.bits + ((size_t)i * hp.max_slices + sl) * (kRankCols / 32);
+    long long c = 0;
+    for (int w = threadIdx.x; w < nw; w += BLOCK) c += __popc(g[w]);
+    c = block_sum<BLOCK, long long>(c, tmp);
+    if (threadIdx.x == 0) hp.slice_base[(size_t)i * hp.max_slices + sl] = run;
+    run += c;
+  }
+  if (threadIdx.x == 0) row_nz[hp.rows[i]] = run;
+}
 }  // namespace cas

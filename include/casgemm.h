@@ -148,7 +148,7 @@ typedef struct {
 	                                larger rows take the dense kernels */
 	int32_t esc_form;            /* bucketed ESC kernel of the fused rows and of ESC rows over 4096
 	                                products: 1 keeps column, product index and place per product in
-	                                shared memory, 4 rows per SM [1]; 2 is form 1 with each thread's
+	                                shared memory, 4 rows per SM; 2 [the default] is form 1 with each thread's
 	                                columns held in registers between its histogram and scatter
 	                                passes (B's columns read once) and, for rows whose B rows average
 	                                32 products or more, a warp per B row in the value pass (rows of
