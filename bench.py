@@ -288,6 +288,16 @@ def run_batch_mode(args):
         a, b = res[(name, "per_call")][0], res[(name, "waves")][0]
         assert all(x["digest"] == y["digest"] and x["nnz_c"] == y["nnz_c"] for x, y in zip(a, b)), name
     clocks = sampler.stop()
+    # the bound on any batching: every job's own device time, alone (the four
+    # phases, CUDA events), summed; batching can only remove what lies
+    # between and around those kernels
+    alone = []
+    for A, B in jobs:
+        cc, rt = ctx.spgemm_device(A, B, "hybacc")
+        ctx.free(cc)
+        alone.append(rt["total_time"])
+    alone_s = float(sum(alone))
+    heavy = sorted(alone, reverse=True)
     ctx.close()
 
     def arm(name, mode):
@@ -312,6 +322,12 @@ def run_batch_mode(args):
                                                        / arm("scale_le_13", "per_call")["jobs_per_s"], 3)},
         "gpu_launches": all_w["kernel_launches"],
         "clocks": clocks,
+        "bound": {"alone_device_seconds": round(alone_s, 4),
+                  "jobs_per_s_if_no_overhead": round(len(jobs) / alone_s, 3),
+                  "max_speedup_over_per_call": round(all_p["seconds"] / alone_s, 3),
+                  "heaviest_8_jobs_share": round(sum(heavy[:8]) / alone_s, 3),
+                  "how": "sum over jobs of each job's four phases alone (CUDA events); batching can only "
+                         "remove the host waits and launches between them"},
     }
     print(json.dumps(line), flush=True)
     return 0
