@@ -1097,10 +1097,10 @@ cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* 
       case kNB_Dense: {
         if (!c.b_sorted && c.ncol > kRankCols)
           return set_err(ctx, CAS_ERR_BAD_INPUT, "heavy rows over more than %d columns need B rows sorted by column", kRankCols);
-        // the rows of at least kSplitProducts products (log2 size classes 18 and up) lead the
+        // the rows of at least kSplitProducts products (log2 size classes kSplitLog2 and up) lead the
         // bin's heaviest-first order; they are split across blocks when their scratch fits
         int64_t n_split = 0;
-        for (int k = 0; k <= kHeavyClasses - 1 - 18; ++k) n_split += (int64_t)ctx->h_counts[kSlotHeavy + k];
+        for (int k = 0; k <= kHeavyClasses - 1 - kSplitLog2; ++k) n_split += (int64_t)ctx->h_counts[kSlotHeavy + k];
         n_split = std::min(n_split, n);
         const int64_t max_slices = (c.ncol + kRankCols - 1) / kRankCols;
         n_split = std::min<int64_t>(n_split, kSplitScratch / (max_slices * (kRankCols / 8)));

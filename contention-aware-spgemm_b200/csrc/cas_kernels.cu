@@ -2081,7 +2081,8 @@ k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int
 // their value ranges stay in L2, where the atomics resolve; a single block
 // per row (k_numc_dense) keeps hundreds of rows of megabytes each open at
 // once, and their atomics miss L2.
-constexpr int64_t kSplitProducts = int64_t(1) << 18;
+constexpr int kSplitLog2 = 18;
+constexpr int64_t kSplitProducts = int64_t(1) << kSplitLog2;
 constexpr int64_t kPartProducts = int64_t(1) << 17;
 
 struct HeavyPlan {
