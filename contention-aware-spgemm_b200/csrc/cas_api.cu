@@ -69,7 +69,7 @@ struct cas_ctx {
   bool profile = false;
   bool fuse = true;                        // fused ESC rows (no symbolic pass) in cas_spgemm
   int fused_lo = (int)cas::kFusedLo;       // fused rows: more products than this (up to kFusedHi)
-  bool heavy_split = true;                 // dense rows of 2^18 products or more split across blocks
+  bool heavy_split = true;                 // dense rows of 2^17 products or more split across blocks
   int esc_form = 2;                        // bucketed ESC of rows over 4096 products (fused rows included):
                                            // 1 index form (k_numc_esc_idx), 0 k_numc_esc_msd, 2 the index
                                            // form with the keys in registers between its two key passes
@@ -626,6 +626,7 @@ struct Call {
   // bitmaps of heavy rows kept by the symbolic kernel for the numeric one
   uint32_t* dbits = nullptr;
   int32_t* dslot = nullptr;
+  int saved_slices = 1;  // bitmap slots kept per row in dbits
   // the symbolic phase's split rows: their slice bitmaps, and each row's slot
   // in them (-1 for other rows); kept for the numeric setup of split rows
   uint32_t* hbits = nullptr;
@@ -900,8 +901,18 @@ cas_status launch_symb_bins(cas_ctx* ctx, Call& c, int64_t* row_nz) {
           CAS_TRY(symb_split_heavy(ctx, c, drows, nd, row_nz, s));
         }
         if (nd == 0) break;
-        if ((double)nd * (kRankCols / 8) <= kSavedBitmapBytes) {  // bitmaps kept for the numeric kernel
-          CAS_TRY(dev_alloc(ctx, (void**)&c.dbits, (size_t)nd * (kRankCols / 8)));
+        // bitmaps kept for the numeric kernel: every slice of each row when that fits a quarter
+        // of the free device memory (or kSavedBitmapBytes), else one-slice rows only
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+          cudaGetLastError();
+          free_b = 0;
+        }
+        const double cap = std::max(kSavedBitmapBytes, 0.25 * (double)free_b);
+        const int64_t max_slices = (c.ncol + kRankCols - 1) / kRankCols;
+        c.saved_slices = (double)nd * max_slices * (kRankCols / 8) <= cap ? (int)max_slices : 1;
+        if ((double)nd * c.saved_slices * (kRankCols / 8) <= cap) {
+          CAS_TRY(dev_alloc(ctx, (void**)&c.dbits, (size_t)nd * c.saved_slices * (kRankCols / 8)));
           CAS_TRY(dev_alloc(ctx, (void**)&c.dslot, sizeof(int32_t) * (c.m + 1)));
           CAS_CUDA(ctx, cudaMemsetAsync(c.dslot, 0xFF, sizeof(int32_t) * (c.m + 1), ctx->stream));
           CAS_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
@@ -909,7 +920,7 @@ cas_status launch_symb_bins(cas_ctx* ctx, Call& c, int64_t* row_nz) {
         }
         k_symb_dense<512><<<(unsigned)nd, 512, smem_symb_dense<512>(), s>>>(drows, c.A.csr, c.B.csr, c.ncol,
                                                                              c.b_sorted ? 1 : 0, row_nz, c.dbits,
-                                                                             c.dslot, ctx->d_status);
+                                                                             c.dslot, c.saved_slices, ctx->d_status);
         break;
       }
     }
@@ -1032,8 +1043,8 @@ cas_status launch_heavy_split(cas_ctx* ctx, Call& c, const int32_t* rows, int64_
     CAS_TRY(alloc((void**)&hp.ticket, sizeof(unsigned long long)));
     CAS_CUDA(ctx, cudaMemsetAsync(hp.ticket, 0, sizeof(unsigned long long), s));
     k_dense_setup<512, VIn><<<(unsigned)n, 512, smem_numc_dense<512, VIn>(), s>>>(
-        hp, c.A.csr, c.B.csr, c.ncol, c.b_sorted ? 1 : 0, crp, ccol, cval, c.dbits, c.dslot, c.hbits, c.hslot,
-        ctx->d_status);
+        hp, c.A.csr, c.B.csr, c.ncol, c.b_sorted ? 1 : 0, crp, ccol, cval, c.dbits, c.dslot, c.saved_slices, c.hbits,
+        c.hslot, ctx->d_status);
     CAS_TRY(check_launch(ctx, "k_dense_setup"));
     k_scan_one_block<<<1, 1024, 0, s>>>(hp.nparts, n, hp.parts);
     CAS_TRY(check_launch(ctx, "k_scan_one_block"));
@@ -1109,7 +1120,8 @@ cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* 
         if (n_split > 0) CAS_TRY(launch_heavy_split<VIn>(ctx, c, rows, n_split, crp, ccol, cval, s));
         if (n > n_split)
           k_numc_dense<512, VIn><<<(unsigned)(n - n_split), 512, smem_numc_dense<512, VIn>(), s>>>(
-              rows + n_split, A, B, c.ncol, c.b_sorted ? 1 : 0, crp, ccol, cval, c.dbits, c.dslot, ctx->d_status);
+              rows + n_split, A, B, c.ncol, c.b_sorted ? 1 : 0, crp, ccol, cval, c.dbits, c.dslot, c.saved_slices,
+              ctx->d_status);
         break;
       }
     }

@@ -408,7 +408,7 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_symb_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int32_t b_sorted,
              int64_t* __restrict__ row_nz, uint32_t* __restrict__ saved, int32_t* __restrict__ saved_slot,
-             DevStatus* st) {
+             int saved_slices, DevStatus* st) {
   constexpr int W = kDenseChunkBits / 32;
   extern __shared__ __align__(16) uint8_t smem[];
   uint32_t* bm = reinterpret_cast<uint32_t*>(smem);
@@ -433,8 +433,13 @@ k_symb_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int
     if (bad && !multi) dev_report(st, kDevBadIndex, 3, r);
     __syncthreads();
     for (int i = threadIdx.x; i < nw; i += BLOCK) cnt += __popc(bm[i]);
-    if (saved && hi - lo <= kRankCols) {  // one numeric slice: keep the bitmap for the numeric kernel
-      uint32_t* dst = saved + (size_t)blockIdx.x * (kRankCols / 32);
+    // keep the bitmap for the numeric kernel when the row's slices fit its
+    // saved_slices slots (the symbolic and numeric slices are the same: both
+    // kDenseChunkBits == kRankCols columns from the row's first column)
+    const int nsl = (int)((hi - lo + kRankCols - 1) / kRankCols);
+    if (saved && nsl <= saved_slices) {
+      const int sl = (int)((c0 - lo) / kRankCols);
+      uint32_t* dst = saved + ((size_t)blockIdx.x * saved_slices + sl) * (kRankCols / 32);
       for (int i = threadIdx.x; i < nw; i += BLOCK) dst[i] = bm[i];
       if (threadIdx.x == 0) saved_slot[r] = (int32_t)blockIdx.x;
     }
@@ -1983,7 +1988,8 @@ template <int BLOCK, typename VIn>
 __global__ void __launch_bounds__(BLOCK)
 k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int32_t b_sorted,
              const int64_t* __restrict__ crp, int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval,
-             const uint32_t* __restrict__ saved, const int32_t* __restrict__ saved_slot, DevStatus* st) {
+             const uint32_t* __restrict__ saved, const int32_t* __restrict__ saved_slot, int saved_slices,
+             DevStatus* st) {
   using AT = typename Acc<VIn>::T;
   constexpr int NWORD = kRankCols / 32;
   extern __shared__ __align__(16) uint8_t smem[];
@@ -2000,9 +2006,9 @@ k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int
   for (int64_t s0 = lo; s0 < hi; s0 += kRankCols) {
     const int64_t s1 = hi < s0 + kRankCols ? hi : s0 + kRankCols;
     const int nw = (int)((s1 - s0 + 31) >> 5);
-    const int32_t slot = (!multi && saved_slot) ? saved_slot[r] : -1;
-    if (slot >= 0) {  // the symbolic kernel kept this row's bitmap
-      const uint32_t* src = saved + (size_t)slot * (kRankCols / 32);
+    const int32_t slot = saved_slot ? saved_slot[r] : -1;
+    if (slot >= 0) {  // the symbolic kernel kept this row's bitmaps
+      const uint32_t* src = saved + ((size_t)slot * saved_slices + (s0 - lo) / kRankCols) * (kRankCols / 32);
       for (int i = threadIdx.x; i < nw; i += BLOCK) bm[i] = src[i];
       __syncthreads();
     } else {
@@ -2081,7 +2087,7 @@ k_numc_dense(const int32_t* __restrict__ rows, Csr A, Csr B, int64_t c_ncol, int
 // their value ranges stay in L2, where the atomics resolve; a single block
 // per row (k_numc_dense) keeps hundreds of rows of megabytes each open at
 // once, and their atomics miss L2.
-constexpr int kSplitLog2 = 18;
+constexpr int kSplitLog2 = 17;
 constexpr int64_t kSplitProducts = int64_t(1) << kSplitLog2;
 constexpr int64_t kPartProducts = int64_t(1) << 17;
 
@@ -2150,7 +2156,7 @@ template <int BLOCK, typename VIn>
 __global__ void __launch_bounds__(BLOCK)
 k_dense_setup(HeavyPlan hp, Csr A, Csr B, int64_t c_ncol, int32_t b_sorted, const int64_t* __restrict__ crp,
               int32_t* __restrict__ ccol, typename Acc<VIn>::T* __restrict__ cval, const uint32_t* __restrict__ saved,
-              const int32_t* __restrict__ saved_slot, const uint32_t* __restrict__ sym_bits,
+              const int32_t* __restrict__ saved_slot, int saved_slices, const uint32_t* __restrict__ sym_bits,
               const int32_t* __restrict__ sym_slot, DevStatus* st) {
   using AT = typename Acc<VIn>::T;
   constexpr int NWORD = kRankCols / 32;
@@ -2193,14 +2199,14 @@ k_dense_setup(HeavyPlan hp, Csr A, Csr B, int64_t c_ncol, int32_t b_sorted, cons
     const int64_t s0 = lo + (int64_t)sl * kRankCols;
     const int64_t s1 = hi < s0 + kRankCols ? hi : s0 + kRankCols;
     const int nw = (int)((s1 - s0 + 31) >> 5);
-    const int32_t slot = (!multi && saved_slot) ? saved_slot[r] : -1;
+    const int32_t slot = saved_slot ? saved_slot[r] : -1;
     const int32_t hslot = sym_slot ? sym_slot[r] : -1;  // the symbolic phase's split bitmaps
     if (hslot >= 0) {
       const uint32_t* src = sym_bits + ((size_t)hslot * hp.max_slices + sl) * NWORD;
       for (int w = threadIdx.x; w < nw; w += BLOCK) bm[w] = src[w];
       __syncthreads();
     } else if (slot >= 0) {
-      const uint32_t* src = saved + (size_t)slot * NWORD;
+      const uint32_t* src = saved + ((size_t)slot * saved_slices + sl) * NWORD;
       for (int w = threadIdx.x; w < nw; w += BLOCK) bm[w] = src[w];
       __syncthreads();
     } else {

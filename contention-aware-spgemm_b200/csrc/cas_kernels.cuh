@@ -62,6 +62,7 @@ enum AccumMode : int { kAccHash = 0, kAccEsc = 1, kAccHybrid = 2 };
 
 constexpr int kDenseChunkBits = 1 << 19;   // symbolic bitmap slice: 512 Ki columns (64 KiB)
 constexpr int kRankCols = 1 << 19;         // numeric dense slice: 512 Ki columns (64 + 32 + 8 KiB of bitmap and ranks)
+static_assert(kRankCols == kDenseChunkBits, "the symbolic and numeric slices coincide, so bitmaps carry over");
 
 struct Csr {
   int64_t nrow, ncol;

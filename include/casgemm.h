@@ -154,7 +154,7 @@ typedef struct {
 	                                32 products or more, a warp per B row in the value pass (rows of
 	                                up to 6144 products; larger ones take form 1); 0 keeps column and
 	                                value, 3 rows per SM */
-	int32_t heavy_split;         /* 1: dense rows of 2^18 products or more are split across thread blocks
+	int32_t heavy_split;         /* 1: dense rows of 2^17 products or more are split across thread blocks
 	                                by A-entry ranges, heaviest row first, adding into C by atomics that
 	                                stay in L2 [1]; 0: one block per dense row */
 } cas_tuning;

@@ -1,6 +1,6 @@
 """GPU: the heaviest dense rows split across thread blocks.
 
-Dense rows of 2^18 products or more are cut into parts by A-entry ranges of
+Dense rows of 2^17 products or more are cut into parts by A-entry ranges of
 about equal products; the parts add into C by atomics after one block per
 row has written its columns (cas_tuning.heavy_split).  The output must equal
 the oracle's bit for bit, and the product with the split off: an R-MAT graph
@@ -31,7 +31,7 @@ def test_split_rows_match_oracle(ctx, name):
     P = np.diff(casgemm.row_products_prefix(A, B))
     ref = oracle.oracle_spgemm(A, B, "hybacc")
     nz = np.diff(ref[0])
-    heavy = int(((P >= 1 << 18) & (nz > 4096)).sum())  # dense rows (over 4096 columns) of 2^18 products or more
+    heavy = int(((P >= 1 << 17) & (nz > 4096)).sum())  # dense rows (over 4096 columns) of 2^17 products or more
     assert heavy > 0
     saved = ctx.get_tuning()
     try:
