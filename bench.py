@@ -466,6 +466,8 @@ def main():
                     help="pick the row routing with casgemm.Autotuner (cached in CACHE.json) before timing")
     ap.add_argument("--esc-form", type=int, default=None, choices=[0, 1, 2],
                     help="bucketed ESC kernel form (cas_tuning.esc_form); default: the library's")
+    ap.add_argument("--bin-order", type=int, default=None, choices=[0, 1],
+                    help="numeric bins interleaved (0) or grouped (1) on the streams (cas_tuning.bin_order)")
     ap.add_argument("--heavy-split", type=int, default=None, choices=[0, 1],
                     help="split the heaviest dense rows across blocks (cas_tuning.heavy_split); default: the library's")
     ap.add_argument("--assemble", action="store_true",
@@ -520,6 +522,8 @@ def main():
         ctx.set_tuning(esc_form=args.esc_form)
     if args.heavy_split is not None:
         ctx.set_tuning(heavy_split=args.heavy_split)
+    if args.bin_order is not None:
+        ctx.set_tuning(bin_order=args.bin_order)
     if args.tune:
         tuner = casgemm.Autotuner(ctx, args.tune)
         key = casgemm.Autotuner.key(As, B)

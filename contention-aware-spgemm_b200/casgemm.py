@@ -108,7 +108,7 @@ class CasTuning(ctypes.Structure):
     _fields_ = [
         ("acc_thres", ctypes.c_double), ("fusion", ctypes.c_int32), ("fused_min_products", ctypes.c_int32),
         ("esc_max_products", ctypes.c_int32), ("hash_max_nnz", ctypes.c_int32), ("esc_form", ctypes.c_int32),
-        ("heavy_split", ctypes.c_int32),
+        ("heavy_split", ctypes.c_int32), ("bin_order", ctypes.c_int32),
     ]
 
     def as_dict(self):
@@ -299,7 +299,7 @@ class Context:
         cur.update(kw)
         t = CasTuning(float(cur["acc_thres"]), int(cur["fusion"]), int(cur["fused_min_products"]),
                       int(cur["esc_max_products"]), int(cur["hash_max_nnz"]), int(cur["esc_form"]),
-                      int(cur["heavy_split"]))
+                      int(cur["heavy_split"]), int(cur["bin_order"]))
         self._check(self.lib.cas_set_tuning(self.h, ctypes.byref(t)))
 
     def set_fusion(self, on: bool):
@@ -531,10 +531,10 @@ class Autotuner:
     """
 
     CANDIDATES = ([{"acc_thres": a, "fusion": 1, "fused_min_products": lo, "esc_max_products": e,
-                    "hash_max_nnz": 4096, "esc_form": f, "heavy_split": 1}
+                    "hash_max_nnz": 4096, "esc_form": f, "heavy_split": 1, "bin_order": 0}
                    for a in (1.5, 2.0, 5.0) for lo in (1024, 2048, 3072) for e in (4096, 8192) for f in (2, 1, 0)]
                   + [{"acc_thres": 2.0, "fusion": 0, "fused_min_products": 2048, "esc_max_products": 8192,
-                      "hash_max_nnz": 4096, "esc_form": 1, "heavy_split": 1}])
+                      "hash_max_nnz": 4096, "esc_form": 1, "heavy_split": 1, "bin_order": 0}])
 
     def __init__(self, ctx: "Context", cache_path: Optional[str] = None):
         self.ctx = ctx
@@ -587,7 +587,8 @@ class Autotuner:
         if not cfg:
             return False
         self.ctx.set_tuning(**{k: cfg[k] for k in ("acc_thres", "fusion", "fused_min_products",
-                                                    "esc_max_products", "hash_max_nnz", "esc_form", "heavy_split")
+                                                    "esc_max_products", "hash_max_nnz", "esc_form", "heavy_split",
+                                                    "bin_order")
                                if k in cfg})
         return True
 

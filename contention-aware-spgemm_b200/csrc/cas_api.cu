@@ -70,6 +70,7 @@ struct cas_ctx {
   bool fuse = true;                        // fused ESC rows (no symbolic pass) in cas_spgemm
   int fused_lo = (int)cas::kFusedLo;       // fused rows: more products than this (up to kFusedHi)
   bool heavy_split = true;                 // dense rows of 2^17 products or more split across blocks
+  int bin_order = 0;                       // 0: contended and ESC bins interleaved on the streams; 1: grouped
   int esc_form = 2;                        // bucketed ESC of rows over 4096 products (fused rows included):
                                            // 1 index form (k_numc_esc_idx), 0 k_numc_esc_msd, 2 the index
                                            // form with the keys in registers between its two key passes
@@ -902,13 +903,14 @@ cas_status launch_symb_bins(cas_ctx* ctx, Call& c, int64_t* row_nz) {
         }
         if (nd == 0) break;
         // bitmaps kept for the numeric kernel: every slice of each row when that fits a quarter
-        // of the free device memory (or kSavedBitmapBytes), else one-slice rows only
+        // of the free device memory, at most 24 GiB (and at least kSavedBitmapBytes), else
+        // one-slice rows only
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
           cudaGetLastError();
           free_b = 0;
         }
-        const double cap = std::max(kSavedBitmapBytes, 0.25 * (double)free_b);
+        const double cap = std::max(kSavedBitmapBytes, std::min(24.0 * (1ull << 30), 0.25 * (double)free_b));
         const int64_t max_slices = (c.ncol + kRankCols - 1) / kRankCols;
         c.saved_slices = (double)nd * max_slices * (kRankCols / 8) <= cap ? (int)max_slices : 1;
         if ((double)nd * c.saved_slices * (kRankCols / 8) <= cap) {
@@ -1069,14 +1071,26 @@ cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* 
   ctx->stats.split_rows = 0;
   int64_t off[kNumcBins + 1] = {0};
   for (int b = 0; b < kNumcBins; ++b) off[b + 1] = off[b] + c.numc_count[b];
-  const int order[] = {kNB_Dense, kNB_E8K, kNB_H4K, kNB_E6K, kNB_E5K, kNB_E4K, kNB_E3K, kNB_H1K,
-                       kNB_E2K, kNB_E1K, kNB_H256, kNB_Tiny};
+  // bins in launch order, taken round-robin by the auxiliary streams.  The
+  // default interleaves the bins of contended rows (dense and hash: many
+  // products per output column, high cf) with the ESC bins (cf near 1), so
+  // that each stream's neighbours run the other kind at the same time, the
+  // GPU form of the reference's high- and low-contention thread groups
+  // claiming morsels from the two ends of the cf-sorted queue
+  // (src/ams/ams_utils.c:190-216, 697-736).  bin_order 1 launches the
+  // contended bins first and the ESC bins after them.
+  const int interleaved[] = {kNB_Dense, kNB_E8K, kNB_H4K, kNB_E6K, kNB_E5K, kNB_E4K, kNB_E3K, kNB_H1K,
+                             kNB_E2K, kNB_E1K, kNB_H256, kNB_Tiny};
+  const int grouped[] = {kNB_Dense, kNB_H4K, kNB_H1K, kNB_H256, kNB_E8K, kNB_E6K, kNB_E5K, kNB_E4K,
+                         kNB_E3K, kNB_E2K, kNB_E1K, kNB_Tiny};
+  const int* order = ctx->bin_order == 1 ? grouped : interleaved;
   unsigned int* ovf_count = reinterpret_cast<unsigned int*>(ctx->d_counts + kSlotOvf);
   if (!c.ovf_preset) CAS_CUDA(ctx, cudaMemsetAsync(ovf_count, 0, sizeof(unsigned int), ctx->stream));
   CAS_TRY(fork(ctx));
   int64_t esc_rows = c.nf;  // fused rows may have handed rows to the radix-sort kernel too
   int si = 0;
-  for (int b : order) {
+  for (int oi = 0; oi < 12; ++oi) {
+    const int b = order[oi];
     const int64_t n = c.numc_count[b];
     if (n == 0) continue;
     const int32_t* rows = c.rows + off[b];
@@ -1449,7 +1463,8 @@ cas_status cas_set_tuning(cas_ctx* ctx, const cas_tuning* t) {
   if (!ctx || !t) return CAS_ERR_BAD_INPUT;
   if (!(t->acc_thres >= 0.0) || t->fused_min_products < 32 || t->fused_min_products >= (int)cas::kFusedHi ||
       t->esc_max_products < 32 || t->esc_max_products > 8192 || t->hash_max_nnz < 0 || t->hash_max_nnz > 4096 ||
-      t->esc_form < 0 || t->esc_form > 2 || (t->heavy_split != 0 && t->heavy_split != 1))
+      t->esc_form < 0 || t->esc_form > 2 || (t->heavy_split != 0 && t->heavy_split != 1) ||
+      (t->bin_order != 0 && t->bin_order != 1))
     return set_err(ctx, CAS_ERR_BAD_INPUT, "tuning out of range");
   ctx->acc_thres = t->acc_thres;
   ctx->fuse = t->fusion != 0;
@@ -1458,6 +1473,7 @@ cas_status cas_set_tuning(cas_ctx* ctx, const cas_tuning* t) {
   ctx->hash_max = t->hash_max_nnz;
   ctx->esc_form = t->esc_form;
   ctx->heavy_split = t->heavy_split != 0;
+  ctx->bin_order = t->bin_order;
   return CAS_OK;
 }
 
@@ -1470,6 +1486,7 @@ cas_status cas_get_tuning(const cas_ctx* ctx, cas_tuning* t) {
   t->hash_max_nnz = ctx->hash_max;
   t->esc_form = ctx->esc_form;
   t->heavy_split = ctx->heavy_split ? 1 : 0;
+  t->bin_order = ctx->bin_order;
   return CAS_OK;
 }
 

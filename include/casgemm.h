@@ -157,6 +157,11 @@ typedef struct {
 	int32_t heavy_split;         /* 1: dense rows of 2^17 products or more are split across thread blocks
 	                                by A-entry ranges, heaviest row first, adding into C by atomics that
 	                                stay in L2 [1]; 0: one block per dense row */
+	int32_t bin_order;           /* 0: the numeric bins of contended rows (dense, hash) and of ESC rows
+	                                launch interleaved on the auxiliary streams, so they run side by
+	                                side, as the reference's high- and low-contention thread groups
+	                                claim morsels from the two ends of its cf-sorted queue
+	                                (src/ams/ams_utils.c:190-216) [0]; 1: contended bins first */
 } cas_tuning;
 cas_status cas_set_tuning(cas_ctx *ctx, const cas_tuning *t);
 cas_status cas_get_tuning(const cas_ctx *ctx, cas_tuning *t);

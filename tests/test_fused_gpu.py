@@ -185,7 +185,8 @@ def test_tuning_routes_rows_but_not_results(ctx):
     seen = set()
     try:
         for kw in ({"esc_max_products": 1024}, {"hash_max_nnz": 256}, {"fused_min_products": 512},
-                   {"acc_thres": 5.0}, {"fusion": 0}, {"esc_form": 0}, {"esc_form": 0, "fused_min_products": 512}):
+                   {"acc_thres": 5.0}, {"fusion": 0}, {"esc_form": 0}, {"esc_form": 0, "fused_min_products": 512},
+                   {"bin_order": 1}, {"heavy_split": 0}):
             ctx.set_tuning(**saved)
             ctx.set_tuning(**kw)
             out = ctx.spgemm(A, B, "hybacc")
