@@ -636,7 +636,7 @@ def main():
     form = ctx.get_tuning().get("esc_form", 1)
     idx_form = form >= 1
     if dom == "fused":
-        kernel_name = "k_numc_esc_%s<256,4800,11,fused%s>" % ("idx" if idx_form else "msd",
+        kernel_name = "k_numc_esc_%s<256,5120,11,fused%s>" % ("idx" if idx_form else "msd",
                                                             ",keys in registers" if form == 2 else "")
     if kernel_name is None and dom.startswith("esc"):
         shape = {"esc1k": "1024,9", "esc2k": "2048,9", "esc3k": "3072,10", "esc4k": "4096,10",

@@ -531,10 +531,12 @@ class Autotuner:
     """
 
     CANDIDATES = ([{"acc_thres": a, "fusion": 1, "fused_min_products": lo, "esc_max_products": e,
-                    "hash_max_nnz": 4096, "esc_form": f, "heavy_split": 1, "bin_order": 0}
+                    "hash_max_nnz": 4096, "esc_form": f, "heavy_split": 1, "bin_order": 1}
                    for a in (1.5, 2.0, 5.0) for lo in (1024, 2048, 3072) for e in (4096, 8192) for f in (2, 1, 0)]
                   + [{"acc_thres": 2.0, "fusion": 0, "fused_min_products": 2048, "esc_max_products": 8192,
-                      "hash_max_nnz": 4096, "esc_form": 1, "heavy_split": 1, "bin_order": 0}])
+                      "hash_max_nnz": 4096, "esc_form": 1, "heavy_split": 1, "bin_order": 1},
+                     {"acc_thres": 2.0, "fusion": 1, "fused_min_products": 2048, "esc_max_products": 8192,
+                      "hash_max_nnz": 4096, "esc_form": 2, "heavy_split": 1, "bin_order": 0}])
 
     def __init__(self, ctx: "Context", cache_path: Optional[str] = None):
         self.ctx = ctx

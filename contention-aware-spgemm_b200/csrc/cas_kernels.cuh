@@ -75,7 +75,7 @@ struct Csr {
 // when fusion is on (fuse_lo > 0; the default lower bound is kFusedLo): no
 // symbolic pass, so they sit in the symbolic zero bin.
 constexpr int64_t kFusedLo = 2048;
-constexpr int64_t kFusedHi = 4800;
+constexpr int64_t kFusedHi = 5120;
 __host__ __device__ __forceinline__ bool fused_row(int64_t flp, int fuse_lo) {
   return fuse_lo > 0 && flp > fuse_lo && flp <= kFusedHi;
 }

@@ -125,7 +125,7 @@ cas_status cas_set_stream(cas_ctx *ctx, void *stream);
 cas_status cas_set_acc_thres(cas_ctx *ctx, double thres);
 const char *cas_last_error(const cas_ctx *ctx);
 /* 1 (default): in cas_spgemm with the ESC or hybrid accumulator, rows of
- * 2049..4800 products (the lower bound is cas_tuning.fused_min_products)
+ * 2049..5120 products (the lower bound is cas_tuning.fused_min_products)
  * skip the symbolic pass: one kernel counts, sorts and
  * places each of them, finding its offset in C from the rows before it, and
  * C is allocated by the bound min(products, columns) for those rows
@@ -142,7 +142,7 @@ cas_status cas_set_fusion(cas_ctx *ctx, int on);
 typedef struct {
 	double acc_thres;            /* AMS_ACC_THRES of the hybrid accumulator [2.0] */
 	int32_t fusion;              /* fused ESC rows, as cas_set_fusion [1] */
-	int32_t fused_min_products;  /* fused rows have more products than this, up to 4800 [2048] */
+	int32_t fused_min_products;  /* fused rows have more products than this, up to 5120 [2048] */
 	int32_t esc_max_products;    /* ESC rows have at most this many products, <= 8192 [8192] */
 	int32_t hash_max_nnz;        /* hash rows have at most this many distinct columns, <= 4096 [4096];
 	                                larger rows take the dense kernels */
@@ -157,11 +157,11 @@ typedef struct {
 	int32_t heavy_split;         /* 1: dense rows of 2^17 products or more are split across thread blocks
 	                                by A-entry ranges, heaviest row first, adding into C by atomics that
 	                                stay in L2 [1]; 0: one block per dense row */
-	int32_t bin_order;           /* 0: the numeric bins of contended rows (dense, hash) and of ESC rows
-	                                launch interleaved on the auxiliary streams, so they run side by
-	                                side, as the reference's high- and low-contention thread groups
-	                                claim morsels from the two ends of its cf-sorted queue
-	                                (src/ams/ams_utils.c:190-216) [0]; 1: contended bins first */
+	int32_t bin_order;           /* 1: the numeric bins of contended rows (dense, hash) launch first on
+	                                the auxiliary streams, the ESC bins after them [1]; 0: the two
+	                                kinds interleaved, so they run side by side, as the reference's
+	                                high- and low-contention thread groups claim morsels from the two
+	                                ends of its cf-sorted queue (src/ams/ams_utils.c:190-216) */
 } cas_tuning;
 cas_status cas_set_tuning(cas_ctx *ctx, const cas_tuning *t);
 cas_status cas_get_tuning(const cas_ctx *ctx, cas_tuning *t);

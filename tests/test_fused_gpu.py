@@ -1,6 +1,6 @@
 """GPU: the fused ESC rows (no symbolic pass, offsets by look-back).
 
-Rows of 2049..4800 products are counted, sorted and placed by one kernel in
+Rows of 2049..5120 products are counted, sorted and placed by one kernel in
 row order, in its index form (column and product index in shared memory) or
 its column-and-value form.  Checked bit for bit against the oracle and against the same
 product with fusion off: uniform rows (nearly all fused), rows whose
@@ -186,7 +186,7 @@ def test_tuning_routes_rows_but_not_results(ctx):
     try:
         for kw in ({"esc_max_products": 1024}, {"hash_max_nnz": 256}, {"fused_min_products": 512},
                    {"acc_thres": 5.0}, {"fusion": 0}, {"esc_form": 0}, {"esc_form": 0, "fused_min_products": 512},
-                   {"bin_order": 1}, {"heavy_split": 0}):
+                   {"bin_order": 0}, {"heavy_split": 0}):
             ctx.set_tuning(**saved)
             ctx.set_tuning(**kw)
             out = ctx.spgemm(A, B, "hybacc")
@@ -270,7 +270,7 @@ def _hot_long_rows(seed=8, ncol=3000, per_row=80, blen=40, hot=2):
 
 def _register_form_cases():
     er = casgemm.gen_er(13, 32, 7)
-    er_wide = casgemm.gen_er(12, 40, 3)   # rows of 4801..6144 products: the 6144 bin
+    er_wide = casgemm.gen_er(12, 40, 3)   # rows of 5121..6144 products: the 6144 bin
     g500 = casgemm.gen_g500(12, 16, 5)   # short B rows: the product-order value pass
     hotA, hotB = hot_column_matrix(per_row=120, hot=2)
     longA, longB = _hot_long_rows()
