@@ -466,6 +466,8 @@ def main():
                     help="pick the row routing with casgemm.Autotuner (cached in CACHE.json) before timing")
     ap.add_argument("--esc-form", type=int, default=None, choices=[0, 1, 2],
                     help="bucketed ESC kernel form (cas_tuning.esc_form); default: the library's")
+    ap.add_argument("--out-blocks", type=int, default=None,
+                    help="row blocks of the e2e leg's host C (cas_tuning.out_blocks; 0 by size, 1 one block)")
     ap.add_argument("--bin-order", type=int, default=None, choices=[0, 1],
                     help="numeric bins interleaved (0) or grouped (1) on the streams (cas_tuning.bin_order)")
     ap.add_argument("--heavy-split", type=int, default=None, choices=[0, 1],
@@ -524,6 +526,8 @@ def main():
         ctx.set_tuning(heavy_split=args.heavy_split)
     if args.bin_order is not None:
         ctx.set_tuning(bin_order=args.bin_order)
+    if args.out_blocks is not None:
+        ctx.set_tuning(out_blocks=args.out_blocks)
     if args.tune:
         tuner = casgemm.Autotuner(ctx, args.tune)
         key = casgemm.Autotuner.key(As, B)
@@ -704,6 +708,7 @@ def main():
                 walls.append(time.perf_counter() - tw)
             s = ctx.stats()
             h2d, d2h, d2h_direct = s["h2d_bytes"], s["d2h_bytes"], s["d2h_direct_bytes"]
+            out_blocks = s["out_blocks"]
             ctx.lib.cas_csr_free(ctx.h, ctypes.byref(cc))
         wall = statistics.mean(walls)
         if dist:
@@ -713,10 +718,11 @@ def main():
         line["e2e"] = {"value": round(2.0 * P_total / wall / 1e9, 3), "unit": "GFLOP/s",
                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                        "steps": args.e2e_steps, "s_per_step": round(wall, 3),
-                       "warmup": 1, "d2h_direct_bytes_per_step": d2h_direct,
+                       "warmup": 1, "d2h_direct_bytes_per_step": d2h_direct, "out_blocks": out_blocks,
                        "path": "cas_spgemm on pinned host A, B; C returned in host memory (after one untimed "
                                "call, so C's host blocks are the context's resident ones, registered with "
-                               "CUDA when they came back; d2h_direct bytes went to them by DMA directly)"}
+                               "CUDA when they came back; d2h_direct bytes went to them by DMA directly), "
+                               "computed in out_blocks row blocks, each copied out while the next is computed"}
         del hA, hB
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

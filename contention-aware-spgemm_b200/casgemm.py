@@ -57,6 +57,7 @@ class CasStats(ctypes.Structure):
         ("esc_overflow_rows", ctypes.c_int64), ("esc_overflow_ms", ctypes.c_double),
         ("fused_rows", ctypes.c_int64), ("fused_flop", ctypes.c_int64), ("fused_bytes", ctypes.c_double),
         ("fused_ms", ctypes.c_double), ("d2h_direct_bytes", ctypes.c_double), ("split_rows", ctypes.c_int64),
+        ("out_blocks", ctypes.c_int64),
     ]
 
 
@@ -108,7 +109,7 @@ class CasTuning(ctypes.Structure):
     _fields_ = [
         ("acc_thres", ctypes.c_double), ("fusion", ctypes.c_int32), ("fused_min_products", ctypes.c_int32),
         ("esc_max_products", ctypes.c_int32), ("hash_max_nnz", ctypes.c_int32), ("esc_form", ctypes.c_int32),
-        ("heavy_split", ctypes.c_int32), ("bin_order", ctypes.c_int32),
+        ("heavy_split", ctypes.c_int32), ("bin_order", ctypes.c_int32), ("out_blocks", ctypes.c_int32),
     ]
 
     def as_dict(self):
@@ -299,7 +300,7 @@ class Context:
         cur.update(kw)
         t = CasTuning(float(cur["acc_thres"]), int(cur["fusion"]), int(cur["fused_min_products"]),
                       int(cur["esc_max_products"]), int(cur["hash_max_nnz"]), int(cur["esc_form"]),
-                      int(cur["heavy_split"]), int(cur["bin_order"]))
+                      int(cur["heavy_split"]), int(cur["bin_order"]), int(cur["out_blocks"]))
         self._check(self.lib.cas_set_tuning(self.h, ctypes.byref(t)))
 
     def set_fusion(self, on: bool):
@@ -326,6 +327,7 @@ class Context:
             "esc_overflow_rows": s.esc_overflow_rows, "esc_overflow_ms": s.esc_overflow_ms,
             "fused_rows": s.fused_rows, "fused_flop": s.fused_flop, "fused_bytes": s.fused_bytes,
             "fused_ms": s.fused_ms, "d2h_direct_bytes": s.d2h_direct_bytes, "split_rows": s.split_rows,
+            "out_blocks": s.out_blocks,
         }
 
     def spgemm(self, A, B, accum: str = "hybacc", col_bytes: int = 4) -> Result:

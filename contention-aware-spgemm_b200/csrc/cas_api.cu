@@ -26,6 +26,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <string>
 #include <vector>
 
@@ -35,7 +36,11 @@
 namespace {
 
 constexpr int kAux = 4;          // auxiliary streams for concurrent bins
+constexpr int kMaxOutBlocks = 64;  // row blocks of a C returned in host memory, at most
+constexpr double kOutBlockMin = double(1ull << 30);    // host C under this: one block
+constexpr double kOutBlockBytes = double(2ull << 30);  // else a block per this many bytes of C
 constexpr int kCountSlots = 256; // device/pinned counter block
+constexpr int kMiscWords = 8;    // pinned words of other small results
 
 // Layout of the counter block (unsigned long long slots).
 constexpr int kSlotSymb = 0;     // [0, 9)   symbolic bin counts
@@ -76,8 +81,10 @@ struct cas_ctx {
                                            // form with the keys in registers between its two key passes
   int esc_max = 8192;                      // ESC rows: at most this many products
   int hash_max = 4096;                     // hash rows: at most this many distinct columns
+  int out_blocks = 0;                      // C in host memory: row blocks (0: by C's size)
   double acc_thres = 2.0;
   cudaEvent_t ev_fused[2] = {};
+  cudaStream_t copy_stream = nullptr;      // copies of finished row blocks of a host C
   std::string err;
   cas_stats stats{};
   int64_t launches = 0;
@@ -85,6 +92,11 @@ struct cas_ctx {
   unsigned long long* d_counts = nullptr;
   unsigned long long* h_counts = nullptr;  // pinned mirror
   cas::DevStatus* h_status = nullptr;      // pinned mirror
+  unsigned long long* h_misc = nullptr;    // pinned words for other small results
+  // the mirrors' device-side addresses (the device writes them by k_fetch_words)
+  unsigned long long* h_counts_dev = nullptr;
+  unsigned long long* h_status_dev = nullptr;
+  unsigned long long* h_misc_dev = nullptr;
   void* h_stage[3] = {};                   // pinned staging for large host copies
   cudaEvent_t ev_stage[3] = {};
   // host blocks of returned C arrays: capacity of every live block this
@@ -148,9 +160,17 @@ const char* dev_err_name(int code) {
   }
 }
 
+// n words (8 bytes each) from device memory into a pinned mirror, written
+// by a one-block kernel on s through the mirror's device-side address
+// (mirror_dev); the caller synchronises s before reading the mirror.
+static_assert(sizeof(cas::DevStatus) % 8 == 0, "the status is fetched in 8-byte words");
+cas_status fetch_words(cas_ctx* ctx, unsigned long long* mirror_dev, const void* src, int n, cudaStream_t s) {
+  cas::k_fetch_words<<<1, 256, 0, s>>>(mirror_dev, static_cast<const unsigned long long*>(src), n);
+  return check_launch(ctx, "k_fetch_words");
+}
+
 cas_status check_status(cas_ctx* ctx) {
-  CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(cas::DevStatus), cudaMemcpyDeviceToHost,
-                                ctx->stream));
+  CAS_TRY(fetch_words(ctx, ctx->h_status_dev, ctx->d_status, (int)(sizeof(cas::DevStatus) / 8), ctx->stream));
   CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (ctx->h_status->err != 0) {
     return set_err(ctx, CAS_ERR_DEVICE, "device check failed in kernel %d at row %lld: %s", ctx->h_status->kernel,
@@ -694,36 +714,42 @@ cas_status launch_scan(cas_ctx* ctx, int64_t* out, const int64_t* in, int64_t n,
 }
 
 // ------------------------------------------------------------------ INIT
+// Row pointers and column indices of A and B in range (an error if not), and
+// whether B's rows are sorted by column (c.b_sorted).  Synchronises.
+cas_status check_inputs(cas_ctx* ctx, Call& c) {
+  using namespace cas;
+  CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_counts + kSlotCheck, 0, sizeof(unsigned long long) * 4, ctx->stream));
+  const int g = grid_for(std::max<int64_t>(c.A.csr.nrow, c.B.csr.nrow) * 32, 256, ctx->sm_count * 16);
+  Csr a = c.A.csr;
+  a.ncol = c.B.csr.nrow;  // A's columns index B's rows
+  k_check_csr<<<g, 256, 0, ctx->stream>>>(a, c.A.nnz, ctx->d_counts + kSlotCheck);
+  CAS_TRY(check_launch(ctx, "k_check_csr"));
+  k_check_csr<<<g, 256, 0, ctx->stream>>>(c.B.csr, c.B.nnz, ctx->d_counts + kSlotCheck + 2);
+  CAS_TRY(check_launch(ctx, "k_check_csr"));
+  CAS_TRY(fetch_words(ctx, ctx->h_counts_dev + kSlotCheck, ctx->d_counts + kSlotCheck, 4, ctx->stream));
+  CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ctx->h_counts[kSlotCheck] || ctx->h_counts[kSlotCheck + 2])
+    return set_err(ctx, CAS_ERR_BAD_INPUT, "invalid CSR input: row pointers or column indices out of range");
+  c.b_sorted = ctx->h_counts[kSlotCheck + 3] == 0;
+  return CAS_OK;
+}
+
+// With `validate`, checks the inputs first (check_inputs); without, c.b_sorted
+// is the caller's (a row block of a checked product).
 cas_status phase_init(cas_ctx* ctx, Call& c, bool validate) {
   using namespace cas;
+  if (validate) CAS_TRY(check_inputs(ctx, c));
   CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_counts, 0, sizeof(unsigned long long) * kCountSlots, ctx->stream));
   CAS_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(DevStatus), ctx->stream));
   CAS_TRY(scratch_alloc(ctx, c));
-  if (validate) {
-    const int g = grid_for(std::max<int64_t>(c.A.csr.nrow, c.B.csr.nrow) * 32, 256, ctx->sm_count * 16);
-    Csr a = c.A.csr;
-    a.ncol = c.B.csr.nrow;  // A's columns index B's rows
-    k_check_csr<<<g, 256, 0, ctx->stream>>>(a, c.A.nnz, ctx->d_counts + kSlotCheck);
-    CAS_TRY(check_launch(ctx, "k_check_csr"));
-    k_check_csr<<<g, 256, 0, ctx->stream>>>(c.B.csr, c.B.nnz, ctx->d_counts + kSlotCheck + 2);
-    CAS_TRY(check_launch(ctx, "k_check_csr"));
-  }
   if (c.m > 0) {
     k_flp<256><<<grid_for(c.m * 32, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
         c.A.csr, c.B.csr, c.ncol, c.row_flp, ctx->d_counts + kSlotTotals, ctx->d_counts + kSlotSymb, ctx->d_status,
         c.fuse, ctx->d_counts + kSlotFused);
     CAS_TRY(check_launch(ctx, "k_flp"));
   }
-  CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts, ctx->d_counts, sizeof(unsigned long long) * kCountSlots,
-                                cudaMemcpyDeviceToHost, ctx->stream));
+  CAS_TRY(fetch_words(ctx, ctx->h_counts_dev, ctx->d_counts, kCountSlots, ctx->stream));
   CAS_TRY(check_status(ctx));  // synchronises
-  if (validate) {
-    if (ctx->h_counts[kSlotCheck] || ctx->h_counts[kSlotCheck + 2])
-      return set_err(ctx, CAS_ERR_BAD_INPUT, "invalid CSR input: row pointers or column indices out of range");
-    c.b_sorted = ctx->h_counts[kSlotCheck + 3] == 0;
-  } else {
-    c.b_sorted = false;
-  }
   c.flop = (int64_t)ctx->h_counts[kSlotTotals];
   c.max_flp = (int64_t)ctx->h_counts[kSlotTotals + 1];
   c.nf = (int64_t)ctx->h_counts[kSlotFused];
@@ -827,9 +853,9 @@ cas_status symb_split_heavy(cas_ctx* ctx, Call& c, int32_t*& rows, int64_t& n, i
   k_split_dense_rows<<<grid_for(n, 256, ctx->sm_count * 4), 256, 0, s>>>(rows, n, c.row_flp, cap, heavy, light, counts,
                                                                           c.hslot);
   CAS_TRY(check_launch(ctx, "k_split_dense_rows"));
-  unsigned long long h[2] = {0, 0};
-  CAS_CUDA(ctx, cudaMemcpyAsync(h, counts, sizeof(h), cudaMemcpyDeviceToHost, s));
+  CAS_TRY(fetch_words(ctx, ctx->h_misc_dev, counts, 2, s));
   CAS_CUDA(ctx, cudaStreamSynchronize(s));
+  const unsigned long long h[2] = {ctx->h_misc[0], ctx->h_misc[1]};
   const int64_t nh = std::min<int64_t>((int64_t)h[0], cap);
   rows = light;
   n = (int64_t)h[1];
@@ -947,12 +973,9 @@ cas_status numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int mode) {
         ctx->d_counts + kSlotNumc, ctx->d_counts + kSlotBinSums, ctx->d_counts + kSlotHeavy);
     CAS_TRY(check_launch(ctx, "k_bin_count_numc"));
   }
-  CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotNumc, ctx->d_counts + kSlotNumc,
-                                sizeof(unsigned long long) * kNumcBins, cudaMemcpyDeviceToHost, ctx->stream));
-  CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotBinSums, ctx->d_counts + kSlotBinSums,
-                                sizeof(unsigned long long) * 3 * kNumcBins, cudaMemcpyDeviceToHost, ctx->stream));
-  CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotHeavy, ctx->d_counts + kSlotHeavy,
-                                sizeof(unsigned long long) * kHeavyClasses, cudaMemcpyDeviceToHost, ctx->stream));
+  CAS_TRY(fetch_words(ctx, ctx->h_counts_dev + kSlotNumc, ctx->d_counts + kSlotNumc, kNumcBins, ctx->stream));
+  CAS_TRY(fetch_words(ctx, ctx->h_counts_dev + kSlotBinSums, ctx->d_counts + kSlotBinSums, 3 * kNumcBins, ctx->stream));
+  CAS_TRY(fetch_words(ctx, ctx->h_counts_dev + kSlotHeavy, ctx->d_counts + kSlotHeavy, kHeavyClasses, ctx->stream));
   CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   unsigned long long* cur = ctx->h_counts + kSlotCursor;
   unsigned long long off = 0;
@@ -1180,6 +1203,351 @@ cas_status prepare(cas_ctx* ctx, const cas_csr* A, const cas_csr* B, Call& c, do
   return CAS_OK;
 }
 
+// C of one product in device memory (compute_dev).
+struct DevC {
+  int64_t* crp = nullptr;
+  int32_t* ccol = nullptr;
+  void* cval = nullptr;
+  int64_t nnz = 0, nnz_known = 0;
+};
+
+void free_dev_c(DevC& o, cudaStream_t s) {
+  if (o.crp) cudaFreeAsync(o.crp, s);
+  if (o.ccol) cudaFreeAsync(o.ccol, s);
+  if (o.cval) cudaFreeAsync(o.cval, s);
+  o.crp = nullptr;
+  o.ccol = nullptr;
+  o.cval = nullptr;
+}
+
+// The four phases of one product whose A and B are on the device: C's row
+// pointers, columns and values in device memory (o, nnz exact).  at_cap(cap)
+// runs once C's bound is known and before NUMC is launched (a host output
+// takes its blocks there, while the GPU works).  The phase boundaries are
+// recorded on ev_phase[0..4].
+template <typename F>
+cas_status compute_dev(cas_ctx* ctx, cas_accum accum, Call& c, bool validate, DevC& o, F&& at_cap) {
+  using namespace cas;
+  const size_t vbytes = 8;  // fp64 or int64 output
+  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[0], ctx->stream));
+  // INIT
+  CAS_TRY(phase_init(ctx, c, validate));
+  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[1], ctx->stream));
+  // SYMB
+  CAS_TRY(dev_alloc(ctx, (void**)&o.crp, sizeof(int64_t) * (c.m + 1)));
+  CAS_TRY(launch_symb_bins(ctx, c, c.row_nz));
+  CAS_TRY(launch_scan(ctx, o.crp, c.row_nz, c.m + 1, c.partial,
+                      reinterpret_cast<int64_t*>(ctx->d_counts + kSlotNnz)));
+  CAS_TRY(fetch_words(ctx, ctx->h_counts_dev + kSlotNnz, ctx->d_counts + kSlotNnz, 1, ctx->stream));
+  CAS_TRY(check_status(ctx));
+  // counts of the rows that had a symbolic pass; the fused rows add theirs
+  // in NUMC, within the bound min(products, columns) each
+  o.nnz_known = (int64_t)ctx->h_counts[kSlotNnz];
+  o.nnz = o.nnz_known;
+  const int64_t cap = o.nnz_known + (c.nf > 0 ? c.f_bound : 0);
+  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[2], ctx->stream));
+  // MGMT
+  CAS_TRY(dev_alloc(ctx, (void**)&o.ccol, sizeof(int32_t) * cap));
+  CAS_TRY(dev_alloc(ctx, &o.cval, vbytes * cap));
+  CAS_TRY(at_cap(cap));
+  CAS_TRY(numc_bins(ctx, c, o.crp, mode_of(accum)));
+  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[3], ctx->stream));
+  // NUMC: the fused rows first (they place themselves after the known
+  // counts), then the scan of all counts, which the other kernels write by
+  if (c.nf > 0) {
+    if (c.vt == CAS_VAL_F64) CAS_TRY(launch_fused<double>(ctx, c, o.crp, o.ccol, o.cval, cap));
+    else CAS_TRY(launch_fused<int32_t>(ctx, c, o.crp, o.ccol, o.cval, cap));
+    CAS_TRY(launch_scan(ctx, o.crp, c.row_nz, c.m + 1, c.partial,
+                        reinterpret_cast<int64_t*>(ctx->d_counts + kSlotNnz)));
+  }
+  if (c.vt == CAS_VAL_F64) CAS_TRY(launch_numc_bins<double>(ctx, c, o.crp, o.ccol, o.cval));
+  else CAS_TRY(launch_numc_bins<int32_t>(ctx, c, o.crp, o.ccol, o.cval));
+  CAS_TRY(scratch_free(ctx, c));
+  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[4], ctx->stream));
+  CAS_TRY(fetch_words(ctx, ctx->h_counts_dev + kSlotOvf, ctx->d_counts + kSlotOvf, 1, ctx->stream));
+  CAS_TRY(fetch_words(ctx, ctx->h_counts_dev + kSlotNnz, ctx->d_counts + kSlotNnz, 1, ctx->stream));
+  CAS_TRY(check_status(ctx));
+  o.nnz = (int64_t)ctx->h_counts[kSlotNnz];
+  return CAS_OK;
+}
+
+// The counters of one product just computed (its phases' events and counts
+// are still in the context); kernel launches and copied bytes are the
+// caller's.
+cas_stats product_stats(cas_ctx* ctx, const Call& c, const DevC& o) {
+  using namespace cas;
+  cas_stats s{};
+  s.flop = c.flop;
+  s.max_row_flp = c.max_flp;
+  s.nnz_c = o.nnz;
+  for (int b = 0; b < kSymbBins; ++b) s.symb_bin_rows[b] = c.symb_count[b];
+  for (int b = 0; b < kNumcBins; ++b) s.numc_bin_rows[b] = c.numc_count[b];
+  const double vin = c.vt == CAS_VAL_F64 ? 8.0 : 4.0;
+  for (int b = 0; b < kNumcBins; ++b) {
+    const double flp = (double)ctx->h_counts[kSlotBinSums + b];
+    const double nzc = (double)ctx->h_counts[kSlotBinSums + kNumcBins + b];
+    const double nza = (double)ctx->h_counts[kSlotBinSums + 2 * kNumcBins + b];
+    s.numc_bin_flop[b] = (int64_t)ctx->h_counts[kSlotBinSums + b];
+    s.numc_bin_bytes[b] = (4 + vin) * (nza + flp) + 12.0 * nzc + 16.0 * (double)c.numc_count[b];
+    float ms = 0;
+    if (ctx->profile && b != kNB_Zero && c.numc_count[b] > 0 &&
+        cudaEventElapsedTime(&ms, ctx->ev_numc[0][b], ctx->ev_numc[1][b]) == cudaSuccess)
+      s.numc_bin_ms[b] = ms;
+  }
+  s.fused_rows = c.nf;
+  s.fused_flop = c.f_flop;
+  if (c.nf > 0) {
+    // nnz(C) of the fused rows: all entries less those of the rows with a symbolic pass
+    s.fused_bytes = (4 + vin) * ((double)c.f_nnza + (double)c.f_flop) + 12.0 * (double)(o.nnz - o.nnz_known) +
+                    16.0 * (double)c.nf;
+    float ms = 0;
+    if (ctx->profile && cudaEventElapsedTime(&ms, ctx->ev_fused[0], ctx->ev_fused[1]) == cudaSuccess) s.fused_ms = ms;
+  }
+  s.esc_overflow_rows = (int64_t)(ctx->h_counts[kSlotOvf] & 0xFFFFFFFFull);
+  {
+    float ms = 0;
+    if (ctx->profile && c.ovf_launched && cudaEventElapsedTime(&ms, ctx->ev_ovf[0], ctx->ev_ovf[1]) == cudaSuccess)
+      s.esc_overflow_ms = ms;
+  }
+  for (int b = 0; b < kSymbBins; ++b) {
+    float ms = 0;
+    if (ctx->profile && b != kSB_Zero && c.symb_count[b] > 0 &&
+        cudaEventElapsedTime(&ms, ctx->ev_symb[0][b], ctx->ev_symb[1][b]) == cudaSuccess)
+      s.symb_bin_ms[b] = ms;
+  }
+  s.split_rows = ctx->stats.split_rows;  // set by this product's launch_numc_bins
+  s.out_blocks = 1;
+  cudaGetLastError();  // leave no error pending from the timing queries
+  return s;
+}
+
+// a += b for the counters of two row blocks of one product
+void add_stats(cas_stats& a, const cas_stats& b) {
+  a.flop += b.flop;
+  a.max_row_flp = std::max(a.max_row_flp, b.max_row_flp);
+  a.nnz_c += b.nnz_c;
+  for (int i = 0; i < CAS_SYMB_BINS; ++i) {
+    a.symb_bin_rows[i] += b.symb_bin_rows[i];
+    a.symb_bin_ms[i] += b.symb_bin_ms[i];
+  }
+  for (int i = 0; i < CAS_NUMC_BINS; ++i) {
+    a.numc_bin_rows[i] += b.numc_bin_rows[i];
+    a.numc_bin_ms[i] += b.numc_bin_ms[i];
+    a.numc_bin_bytes[i] += b.numc_bin_bytes[i];
+    a.numc_bin_flop[i] += b.numc_bin_flop[i];
+  }
+  a.esc_overflow_rows += b.esc_overflow_rows;
+  a.esc_overflow_ms += b.esc_overflow_ms;
+  a.fused_rows += b.fused_rows;
+  a.fused_flop += b.fused_flop;
+  a.fused_bytes += b.fused_bytes;
+  a.fused_ms += b.fused_ms;
+  a.split_rows += b.split_rows;
+  a.out_blocks += b.out_blocks;
+}
+
+void phase_times(cas_ctx* ctx, double t[4]) {
+  for (int i = 0; i < 4; ++i) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, ctx->ev_phase[i], ctx->ev_phase[i + 1]) == cudaSuccess) t[i] += ms * 1e-3;
+  }
+  cudaGetLastError();
+}
+
+// The sum over A's rows of min(products, columns), an upper bound on nnz(C).
+cas_status nnz_bound(cas_ctx* ctx, const Call& c, int64_t& bound) {
+  using namespace cas;
+  unsigned long long* d = ctx->d_counts + kSlotNnz;
+  CAS_CUDA(ctx, cudaMemsetAsync(d, 0, sizeof(unsigned long long), ctx->stream));
+  if (c.m > 0) {
+    k_nnz_bound<256><<<grid_for(c.m * 32, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(c.A.csr, c.B.csr, c.ncol, d);
+    CAS_TRY(check_launch(ctx, "k_nnz_bound"));
+  }
+  CAS_TRY(fetch_words(ctx, ctx->h_counts_dev + kSlotNnz, d, 1, ctx->stream));
+  CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  bound = (int64_t)ctx->h_counts[kSlotNnz];
+  return CAS_OK;
+}
+
+// C in host memory by row blocks of about equal A entries.  Each block runs
+// the four phases as a product of its own (with its own fused-row tickets)
+// into device memory; its row pointers are moved to its place in C, and the
+// block is copied out on the copy stream, straight into C's host arrays where
+// the context has registered them, while the next block is computed.  The
+// host arrays are sized by `bound` (the sum over rows of min(products,
+// columns)); num_nnz is exact.
+cas_status run_blocked(cas_ctx* ctx, cas_accum accum, const cas_csr* A, Call& full, int nblk, int64_t bound,
+                       cas_csr* C, cas_runtime* rt, double& d2h) {
+  using namespace cas;
+  const size_t vbytes = 8;
+  const int64_t m = full.m;
+  std::vector<int64_t> rb((size_t)nblk + 1);
+  for (int k = 0; k <= nblk; ++k) {
+    if (!A->on_device) {
+      const int64_t target = (int64_t)((double)A->num_nnz * k / nblk);
+      rb[(size_t)k] = std::lower_bound(A->row_ptrs, A->row_ptrs + m + 1, target) - A->row_ptrs;
+    } else {
+      rb[(size_t)k] = m * k / nblk;
+    }
+  }
+  rb[0] = 0;
+  rb[(size_t)nblk] = m;
+  int64_t* h_rp = static_cast<int64_t*>(host_take(ctx, sizeof(int64_t) * (m + 1)));
+  void* h_col = host_take(ctx, sizeof(int32_t) * (size_t)(bound > 0 ? bound : 1));
+  void* h_val = host_take(ctx, vbytes * (size_t)(bound > 0 ? bound : 1));
+  auto free_host = [&] {
+    host_give(ctx, h_rp);
+    host_give(ctx, h_col);
+    host_give(ctx, h_val);
+  };
+  if (!h_rp || !h_col || !h_val) {
+    free_host();
+    return set_err(ctx, CAS_ERR_OOM, "host allocation of C failed");
+  }
+  const bool pin_col = host_is_pinned(ctx, h_col), pin_val = host_is_pinned(ctx, h_val);
+  // C's row pointers gather on the device, each block's moved to its place,
+  // and go out in one copy at the end
+  int64_t* d_rp = nullptr;
+  {
+    const cas_status a = dev_alloc(ctx, (void**)&d_rp, sizeof(int64_t) * (size_t)(m + 1));
+    if (a != CAS_OK) {
+      free_host();
+      return a;
+    }
+  }
+  cudaEvent_t ev_done = nullptr;
+  CAS_CUDA(ctx, cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
+  // A block's device buffers are freed (on the main stream) only once its
+  // copies are seen to be complete: freed in the copy stream's order, the
+  // pool could hand their memory to a later block and make the main stream
+  // wait for the copy, which would serialise computing and copying.
+  struct InFlight {
+    DevC o;
+    cudaEvent_t copied;
+  };
+  std::deque<InFlight> inflight;
+  auto reap = [&](bool wait) {
+    while (!inflight.empty()) {
+      InFlight& f = inflight.front();
+      if (wait) cudaEventSynchronize(f.copied);
+      else if (cudaEventQuery(f.copied) != cudaSuccess) break;
+      free_dev_c(f.o, ctx->stream);
+      cudaEventDestroy(f.copied);
+      inflight.pop_front();
+    }
+    cudaGetLastError();  // a not-ready query leaves no error behind
+  };
+  cas_stats acc{};
+  double t[4] = {0, 0, 0, 0};
+  int64_t base = 0;
+  int nrun = 0;
+  cas_status st = CAS_OK;
+  for (int k = 0; k < nblk && st == CAS_OK; ++k) {
+    const int64_t r0 = rb[(size_t)k], r1 = rb[(size_t)k + 1];
+    if (r1 <= r0) continue;
+    Call ck;
+    ck.A.csr = full.A.csr;
+    ck.A.csr.rp = full.A.csr.rp + r0;
+    ck.A.csr.nrow = r1 - r0;
+    ck.A.nnz = full.A.nnz;
+    ck.A.vt = full.A.vt;
+    ck.B.csr = full.B.csr;
+    ck.B.nnz = full.B.nnz;
+    ck.B.vt = full.B.vt;
+    ck.m = r1 - r0;
+    ck.ncol = full.ncol;
+    ck.vt = full.vt;
+    ck.fuse = full.fuse;
+    ck.b_sorted = full.b_sorted;
+    DevC o;
+    st = compute_dev(ctx, accum, ck, false, o, [](int64_t) { return CAS_OK; });
+    if (st == CAS_OK && o.nnz > bound - base)
+      st = set_err(ctx, CAS_ERR_DEVICE, "row block %d: %lld entries past the output bound", k,
+                   (long long)(base + o.nnz - bound));
+    if (st == CAS_OK) {
+      k_rebase_to<<<grid_for(ck.m + 1, 256, ctx->sm_count * 4), 256, 0, ctx->stream>>>(d_rp + r0, o.crp, ck.m + 1,
+                                                                                        base);
+      st = check_launch(ctx, "k_rebase_to");
+    }
+    if (st != CAS_OK) {
+      scratch_free(ctx, ck);
+      free_dev_c(o, ctx->stream);
+      break;
+    }
+    phase_times(ctx, t);
+    const cas_stats bs = product_stats(ctx, ck, o);
+    if (nrun == 0) acc = bs;
+    else add_stats(acc, bs);
+    ++nrun;
+    // the block's columns and values: arrays the context has not registered
+    // through the staging buffers now, the others by DMA on the copy stream
+    char* col_dst = static_cast<char*>(h_col) + sizeof(int32_t) * (size_t)base;
+    char* val_dst = static_cast<char*>(h_val) + vbytes * (size_t)base;
+    const size_t col_b = sizeof(int32_t) * (size_t)o.nnz, val_b = vbytes * (size_t)o.nnz;
+    if (!pin_col && st == CAS_OK) st = d2h_staged(ctx, col_dst, o.ccol, col_b);
+    if (!pin_val && st == CAS_OK) st = d2h_staged(ctx, val_dst, o.cval, val_b);
+    bool queued = false;  // the copy stream waits for the block and reads its buffers
+    if (st == CAS_OK) {
+      cudaError_t e = cudaEventRecord(ev_done, ctx->stream);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_stream, ev_done, 0);
+      queued = e == cudaSuccess;
+      if (e == cudaSuccess && pin_col && col_b)
+        e = cudaMemcpyAsync(col_dst, o.ccol, col_b, cudaMemcpyDeviceToHost, ctx->copy_stream);
+      if (e == cudaSuccess && pin_val && val_b)
+        e = cudaMemcpyAsync(val_dst, o.cval, val_b, cudaMemcpyDeviceToHost, ctx->copy_stream);
+      if (e != cudaSuccess) st = set_err(ctx, CAS_ERR_CUDA, "copy of row block %d: %s", k, cudaGetErrorString(e));
+      ctx->d2h_direct += (pin_col ? (double)col_b : 0.0) + (pin_val ? (double)val_b : 0.0);
+    }
+    cudaEvent_t copied = nullptr;
+    if (queued && cudaEventCreateWithFlags(&copied, cudaEventDisableTiming) == cudaSuccess &&
+        cudaEventRecord(copied, ctx->copy_stream) == cudaSuccess) {
+      inflight.push_back({o, copied});
+    } else {
+      if (copied) cudaEventDestroy(copied);
+      if (queued) cudaStreamSynchronize(ctx->copy_stream);
+      free_dev_c(o, ctx->stream);
+    }
+    reap(false);
+    d2h += (double)(col_b + val_b);
+    base += o.nnz;
+  }
+  const cudaError_t ce = cudaStreamSynchronize(ctx->copy_stream);
+  reap(true);
+  cudaEventDestroy(ev_done);
+  if (st == CAS_OK && ce != cudaSuccess)
+    st = set_err(ctx, CAS_ERR_CUDA, "copy of C's row blocks: %s", cudaGetErrorString(ce));
+  if (st == CAS_OK) {
+    st = d2h_out(ctx, h_rp, d_rp, sizeof(int64_t) * (size_t)(m + 1));
+    d2h += sizeof(int64_t) * (double)(m + 1);
+  }
+  cudaFreeAsync(d_rp, ctx->stream);
+  if (st == CAS_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+    st = set_err(ctx, CAS_ERR_CUDA, "row blocks: %s", cudaGetErrorString(cudaGetLastError()));
+  if (st != CAS_OK) {
+    free_host();
+    return st;
+  }
+  C->num_row = m;
+  C->num_col = full.ncol;
+  C->num_nnz = base;
+  C->val_type = full.vt;
+  C->owned = 2;
+  C->on_device = 0;
+  C->col_bytes = 4;
+  C->row_ptrs = h_rp;
+  C->cols = h_col;
+  C->rats = h_val;
+  if (rt) {
+    rt->init_time = t[0];
+    rt->symb_time = t[1];
+    rt->mgmt_time = t[2];
+    rt->numc_time = t[3];
+    rt->total_time = t[0] + t[1] + t[2] + t[3];
+  }
+  ctx->stats = acc;
+  return CAS_OK;
+}
+
 cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas_csr* B, cas_csr* C,
                       cas_runtime* rt) {
   using namespace cas;
@@ -1192,31 +1560,37 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
   memset(C, 0, sizeof(*C));
   c.fuse = ctx->fuse && accum != CAS_ACC_HASH ? ctx->fused_lo : 0;
   const size_t vbytes = 8;  // fp64 or int64 output
-  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[0], ctx->stream));
-  // INIT
-  CAS_TRY(phase_init(ctx, c, true));
-  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[1], ctx->stream));
-  // SYMB
-  int64_t* crp = nullptr;
-  CAS_TRY(dev_alloc(ctx, (void**)&crp, sizeof(int64_t) * (c.m + 1)));
-  CAS_TRY(launch_symb_bins(ctx, c, c.row_nz));
-  CAS_TRY(launch_scan(ctx, crp, c.row_nz, c.m + 1, c.partial,
-                      reinterpret_cast<int64_t*>(ctx->d_counts + kSlotNnz)));
-  CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotNnz, ctx->d_counts + kSlotNnz, sizeof(unsigned long long),
-                                cudaMemcpyDeviceToHost, ctx->stream));
-  CAS_TRY(check_status(ctx));
-  // counts of the rows that had a symbolic pass; the fused rows add theirs
-  // in NUMC, within the bound min(products, columns) each
-  const int64_t nnz_known = (int64_t)ctx->h_counts[kSlotNnz];
-  const int64_t cap = nnz_known + (c.nf > 0 ? c.f_bound : 0);
-  int64_t nnz = nnz_known;
-  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[2], ctx->stream));
-  // MGMT
-  int32_t* ccol = nullptr;
-  void* cval = nullptr;
-  CAS_TRY(dev_alloc(ctx, (void**)&ccol, sizeof(int32_t) * cap));
-  CAS_TRY(dev_alloc(ctx, &cval, vbytes * cap));
-  // host C
+  auto finish = [&](cas_status st) -> cas_status {
+    cas_status f1 = free_owned(ctx, c.A), f2 = free_owned(ctx, c.B);
+    if (st == CAS_OK) st = f1 != CAS_OK ? f1 : f2;
+    if (st == CAS_OK) {
+      cas_stats& s = ctx->stats;
+      s.kernel_launches = ctx->launches;
+      s.h2d_bytes = h2d;
+      s.d2h_bytes = d2h;
+      s.d2h_direct_bytes = ctx->d2h_direct;
+    }
+    return st;
+  };
+  // a large C in host memory with int32 columns goes by row blocks, each
+  // copied out while the next is computed (cas_tuning.out_blocks)
+  bool checked = false;
+  if (!c_on_device && c_col_bytes == 4 && ctx->out_blocks != 1 && c.m > 1) {
+    cas_status st = check_inputs(ctx, c);
+    int64_t bound = 0;
+    if (st == CAS_OK) st = nnz_bound(ctx, c, bound);
+    if (st != CAS_OK) return finish(st);
+    checked = true;
+    int64_t nblk = ctx->out_blocks;
+    if (nblk == 0) {
+      const double bytes = (4.0 + (double)vbytes) * (double)bound;
+      nblk = bytes < kOutBlockMin ? 1
+                                  : (int64_t)std::min(std::max(2.0, std::ceil(bytes / kOutBlockBytes)), (double)kMaxOutBlocks);
+    }
+    nblk = std::min(nblk, c.m);
+    if (nblk > 1) return finish(run_blocked(ctx, accum, A, c, (int)nblk, bound, C, rt, d2h));
+  }
+  DevC o;
   int64_t* h_rp = nullptr;
   void *h_col = nullptr, *h_val = nullptr;
   auto free_host = [&] {
@@ -1224,49 +1598,20 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
     host_give(ctx, h_col);
     host_give(ctx, h_val);
   };
-  if (!c_on_device) {
+  cas_status st = compute_dev(ctx, accum, c, !checked, o, [&](int64_t cap) -> cas_status {
+    if (c_on_device) return CAS_OK;
     h_rp = static_cast<int64_t*>(host_take(ctx, sizeof(int64_t) * (c.m + 1)));
-    h_col = host_take(ctx, (size_t)c_col_bytes * (cap > 0 ? cap : 1));
-    h_val = host_take(ctx, vbytes * (cap > 0 ? cap : 1));
-    if (!h_rp || !h_col || !h_val) {
-      free_host();
-      return set_err(ctx, CAS_ERR_OOM, "host allocation of C failed");
-    }
-  }
-  {
-    cas_status st = numc_bins(ctx, c, crp, mode_of(accum));
-    if (st != CAS_OK) { free_host(); return st; }
-  }
-  CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[3], ctx->stream));
-  // NUMC
-  cas_status nst = [&]() -> cas_status {
-    if (c.nf > 0) {
-      // fused rows first (they place themselves after the known counts), then
-      // the scan of all counts, which the other kernels write by
-      if (c.vt == CAS_VAL_F64) CAS_TRY(launch_fused<double>(ctx, c, crp, ccol, cval, cap));
-      else CAS_TRY(launch_fused<int32_t>(ctx, c, crp, ccol, cval, cap));
-      CAS_TRY(launch_scan(ctx, crp, c.row_nz, c.m + 1, c.partial,
-                          reinterpret_cast<int64_t*>(ctx->d_counts + kSlotNnz)));
-    }
-    if (c.vt == CAS_VAL_F64) CAS_TRY(launch_numc_bins<double>(ctx, c, crp, ccol, cval));
-    else CAS_TRY(launch_numc_bins<int32_t>(ctx, c, crp, ccol, cval));
-    CAS_TRY(scratch_free(ctx, c));
-    CAS_CUDA(ctx, cudaEventRecord(ctx->ev_phase[4], ctx->stream));
-    CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotOvf, ctx->d_counts + kSlotOvf, sizeof(unsigned long long),
-                                  cudaMemcpyDeviceToHost, ctx->stream));
-    CAS_CUDA(ctx, cudaMemcpyAsync(ctx->h_counts + kSlotNnz, ctx->d_counts + kSlotNnz, sizeof(unsigned long long),
-                                  cudaMemcpyDeviceToHost, ctx->stream));
-    CAS_TRY(check_status(ctx));
-    nnz = (int64_t)ctx->h_counts[kSlotNnz];
-    CAS_TRY(free_owned(ctx, c.A));
-    CAS_TRY(free_owned(ctx, c.B));
+    h_col = host_take(ctx, (size_t)c_col_bytes * (size_t)(cap > 0 ? cap : 1));
+    h_val = host_take(ctx, vbytes * (size_t)(cap > 0 ? cap : 1));
+    if (!h_rp || !h_col || !h_val) return set_err(ctx, CAS_ERR_OOM, "host allocation of C failed");
     return CAS_OK;
-  }();
-  if (nst != CAS_OK) {
+  });
+  if (st != CAS_OK) {
     free_host();
-    return nst;
+    free_dev_c(o, ctx->stream);
+    return finish(st);
   }
-
+  const int64_t nnz = o.nnz;
   C->num_row = c.m;
   C->num_col = c.ncol;
   C->num_nnz = nnz;
@@ -1275,9 +1620,9 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
   if (c_on_device) {
     C->on_device = 1;
     C->col_bytes = 4;
-    C->row_ptrs = crp;
-    C->cols = ccol;
-    C->rats = cval;
+    C->row_ptrs = o.crp;
+    C->cols = o.ccol;
+    C->rats = o.cval;
   } else {
     C->owned = 2;
     C->on_device = 0;
@@ -1285,74 +1630,30 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
     C->row_ptrs = h_rp;
     C->cols = h_col;
     C->rats = h_val;
-    CAS_TRY(d2h_out(ctx, C->row_ptrs, crp, sizeof(int64_t) * (c.m + 1)));
-    CAS_TRY(d2h_out(ctx, C->rats, cval, vbytes * nnz));
-    CAS_TRY(d2h_out(ctx, C->cols, ccol, sizeof(int32_t) * nnz, c_col_bytes == 8));
+    cas_status cs = d2h_out(ctx, C->row_ptrs, o.crp, sizeof(int64_t) * (c.m + 1));
+    if (cs == CAS_OK) cs = d2h_out(ctx, C->rats, o.cval, vbytes * nnz);
+    if (cs == CAS_OK) cs = d2h_out(ctx, C->cols, o.ccol, sizeof(int32_t) * nnz, c_col_bytes == 8);
     d2h += sizeof(int64_t) * (double)(c.m + 1) + (vbytes + c_col_bytes) * (double)nnz;
-    CAS_CUDA(ctx, cudaFreeAsync(crp, ctx->stream));
-    CAS_CUDA(ctx, cudaFreeAsync(ccol, ctx->stream));
-    CAS_CUDA(ctx, cudaFreeAsync(cval, ctx->stream));
-    CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    free_dev_c(o, ctx->stream);
+    if (cs == CAS_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+      cs = set_err(ctx, CAS_ERR_CUDA, "copy of C: %s", cudaGetErrorString(cudaGetLastError()));
+    if (cs != CAS_OK) {
+      free_host();
+      memset(C, 0, sizeof(*C));
+      return finish(cs);
+    }
   }
-  float ms[4];
-  for (int i = 0; i < 4; ++i) CAS_CUDA(ctx, cudaEventElapsedTime(&ms[i], ctx->ev_phase[i], ctx->ev_phase[i + 1]));
   if (rt) {
-    rt->init_time = ms[0] * 1e-3;
-    rt->symb_time = ms[1] * 1e-3;
-    rt->mgmt_time = ms[2] * 1e-3;
-    rt->numc_time = ms[3] * 1e-3;
-    rt->total_time = rt->init_time + rt->symb_time + rt->mgmt_time + rt->numc_time;
+    double t[4] = {0, 0, 0, 0};
+    phase_times(ctx, t);
+    rt->init_time = t[0];
+    rt->symb_time = t[1];
+    rt->mgmt_time = t[2];
+    rt->numc_time = t[3];
+    rt->total_time = t[0] + t[1] + t[2] + t[3];
   }
-  cas_stats& s = ctx->stats;
-  s.flop = c.flop;
-  s.max_row_flp = c.max_flp;
-  s.nnz_c = nnz;
-  for (int b = 0; b < kSymbBins; ++b) s.symb_bin_rows[b] = c.symb_count[b];
-  for (int b = 0; b < kNumcBins; ++b) s.numc_bin_rows[b] = c.numc_count[b];
-  s.kernel_launches = ctx->launches;
-  s.h2d_bytes = h2d;
-  s.d2h_bytes = d2h;
-  s.d2h_direct_bytes = ctx->d2h_direct;
-  const double vin = c.vt == CAS_VAL_F64 ? 8.0 : 4.0;
-  for (int b = 0; b < kNumcBins; ++b) {
-    const double flp = (double)ctx->h_counts[kSlotBinSums + b];
-    const double nzc = (double)ctx->h_counts[kSlotBinSums + kNumcBins + b];
-    const double nza = (double)ctx->h_counts[kSlotBinSums + 2 * kNumcBins + b];
-    s.numc_bin_flop[b] = (int64_t)ctx->h_counts[kSlotBinSums + b];
-    s.numc_bin_bytes[b] = (4 + vin) * (nza + flp) + 12.0 * nzc + 16.0 * (double)c.numc_count[b];
-    s.numc_bin_ms[b] = 0;
-    float ms = 0;
-    if (ctx->profile && b != kNB_Zero && c.numc_count[b] > 0 &&
-        cudaEventElapsedTime(&ms, ctx->ev_numc[0][b], ctx->ev_numc[1][b]) == cudaSuccess)
-      s.numc_bin_ms[b] = ms;
-  }
-  s.fused_rows = c.nf;
-  s.fused_flop = c.f_flop;
-  s.fused_bytes = 0;
-  s.fused_ms = 0;
-  if (c.nf > 0) {
-    // nnz(C) of the fused rows: all entries less those of the rows with a symbolic pass
-    s.fused_bytes = (4 + vin) * ((double)c.f_nnza + (double)c.f_flop) + 12.0 * (double)(nnz - nnz_known) +
-                    16.0 * (double)c.nf;
-    float ms = 0;
-    if (ctx->profile && cudaEventElapsedTime(&ms, ctx->ev_fused[0], ctx->ev_fused[1]) == cudaSuccess) s.fused_ms = ms;
-  }
-  s.esc_overflow_rows = (int64_t)(ctx->h_counts[kSlotOvf] & 0xFFFFFFFFull);
-  s.esc_overflow_ms = 0;
-  {
-    float ms = 0;
-    if (ctx->profile && c.ovf_launched && cudaEventElapsedTime(&ms, ctx->ev_ovf[0], ctx->ev_ovf[1]) == cudaSuccess)
-      s.esc_overflow_ms = ms;
-  }
-  for (int b = 0; b < kSymbBins; ++b) {
-    s.symb_bin_ms[b] = 0;
-    float ms = 0;
-    if (ctx->profile && b != kSB_Zero && c.symb_count[b] > 0 &&
-        cudaEventElapsedTime(&ms, ctx->ev_symb[0][b], ctx->ev_symb[1][b]) == cudaSuccess)
-      s.symb_bin_ms[b] = ms;
-  }
-  cudaGetLastError();  // leave no error pending from the timing queries
-  return CAS_OK;
+  ctx->stats = product_stats(ctx, c, o);
+  return finish(CAS_OK);
 }
 
 }  // namespace
@@ -1376,6 +1677,7 @@ cas_status cas_create(int device, cas_ctx** out) {
       CAS_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming));
     }
     CAS_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+    CAS_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
     for (int i = 0; i < 5; ++i) CAS_CUDA(ctx, cudaEventCreate(&ctx->ev_phase[i]));
     for (int i = 0; i < 2; ++i) CAS_CUDA(ctx, cudaEventCreate(&ctx->ev_fused[i]));
     for (int i = 0; i < 2; ++i) {
@@ -1387,6 +1689,10 @@ cas_status cas_create(int device, cas_ctx** out) {
     CAS_CUDA(ctx, cudaMalloc(&ctx->d_counts, sizeof(unsigned long long) * kCountSlots));
     CAS_CUDA(ctx, cudaMallocHost(&ctx->h_counts, sizeof(unsigned long long) * kCountSlots));
     CAS_CUDA(ctx, cudaMallocHost(&ctx->h_status, sizeof(cas::DevStatus)));
+    CAS_CUDA(ctx, cudaMallocHost(&ctx->h_misc, sizeof(unsigned long long) * kMiscWords));
+    CAS_CUDA(ctx, cudaHostGetDevicePointer((void**)&ctx->h_counts_dev, ctx->h_counts, 0));
+    CAS_CUDA(ctx, cudaHostGetDevicePointer((void**)&ctx->h_status_dev, ctx->h_status, 0));
+    CAS_CUDA(ctx, cudaHostGetDevicePointer((void**)&ctx->h_misc_dev, ctx->h_misc, 0));
     // keep freed device memory in the stream-ordered pool between calls
     cudaMemPool_t pool;
     CAS_CUDA(ctx, cudaDeviceGetDefaultMemPool(&pool, device));
@@ -1408,6 +1714,10 @@ void cas_destroy(cas_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
+  if (ctx->copy_stream) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
+  }
   for (int i = 0; i < kAux; ++i) {
     if (ctx->aux[i]) cudaStreamDestroy(ctx->aux[i]);
     if (ctx->ev_join[i]) cudaEventDestroy(ctx->ev_join[i]);
@@ -1428,6 +1738,7 @@ void cas_destroy(cas_ctx* ctx) {
   if (ctx->d_counts) cudaFree(ctx->d_counts);
   if (ctx->h_counts) cudaFreeHost(ctx->h_counts);
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
+  if (ctx->h_misc) cudaFreeHost(ctx->h_misc);
   for (int i = 0; i < kStageBufs; ++i) {
     if (ctx->h_stage[i]) cudaFreeHost(ctx->h_stage[i]);
     if (ctx->ev_stage[i]) cudaEventDestroy(ctx->ev_stage[i]);
@@ -1466,7 +1777,7 @@ cas_status cas_set_tuning(cas_ctx* ctx, const cas_tuning* t) {
   if (!(t->acc_thres >= 0.0) || t->fused_min_products < 32 || t->fused_min_products >= (int)cas::kFusedHi ||
       t->esc_max_products < 32 || t->esc_max_products > 8192 || t->hash_max_nnz < 0 || t->hash_max_nnz > 4096 ||
       t->esc_form < 0 || t->esc_form > 2 || (t->heavy_split != 0 && t->heavy_split != 1) ||
-      (t->bin_order != 0 && t->bin_order != 1))
+      (t->bin_order != 0 && t->bin_order != 1) || t->out_blocks < 0 || t->out_blocks > kMaxOutBlocks)
     return set_err(ctx, CAS_ERR_BAD_INPUT, "tuning out of range");
   ctx->acc_thres = t->acc_thres;
   ctx->fuse = t->fusion != 0;
@@ -1476,6 +1787,7 @@ cas_status cas_set_tuning(cas_ctx* ctx, const cas_tuning* t) {
   ctx->esc_form = t->esc_form;
   ctx->heavy_split = t->heavy_split != 0;
   ctx->bin_order = t->bin_order;
+  ctx->out_blocks = t->out_blocks;
   return CAS_OK;
 }
 
@@ -1489,6 +1801,7 @@ cas_status cas_get_tuning(const cas_ctx* ctx, cas_tuning* t) {
   t->esc_form = ctx->esc_form;
   t->heavy_split = ctx->heavy_split ? 1 : 0;
   t->bin_order = ctx->bin_order;
+  t->out_blocks = ctx->out_blocks;
   return CAS_OK;
 }
 

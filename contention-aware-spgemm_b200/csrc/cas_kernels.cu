@@ -64,6 +64,49 @@ k_flp(Csr A, Csr B, int64_t c_ncol, int64_t* __restrict__ row_flp,
   }
 }
 
+// The sum over A's rows of min(products, c_ncol), a bound on nnz(C) that is
+// known before any row is counted (C in host memory by row blocks takes its
+// host arrays by it).  A warp per row; columns outside [0, B.nrow) are
+// skipped (the input check reports them).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_nnz_bound(Csr A, Csr B, int64_t c_ncol, unsigned long long* __restrict__ bound) {
+  __shared__ unsigned long long s_b;
+  if (threadIdx.x == 0) s_b = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * BLOCK) >> 5;
+  unsigned long long my_b = 0;
+  for (int64_t r = ((int64_t)blockIdx.x * BLOCK + threadIdx.x) >> 5; r < A.nrow; r += nw) {
+    long long sum = 0;
+    for (int64_t j = A.rp[r] + lane; j < A.rp[r + 1]; j += 32) {
+      const int32_t k = A.col[j];
+      if ((uint64_t)k < (uint64_t)B.nrow) sum += B.rp[k + 1] - B.rp[k];
+    }
+    sum = warp_sum(sum);
+    my_b += (unsigned long long)(sum < c_ncol ? sum : c_ncol);
+  }
+  if (lane == 0 && my_b) atomicAdd(&s_b, my_b);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_b) atomicAdd(bound, s_b);
+}
+
+// dst[0..n) = src[0..n) + add (a row block's row pointers moved to their
+// place in C's).
+__global__ void k_rebase_to(int64_t* __restrict__ dst, const int64_t* __restrict__ src, int64_t n, int64_t add) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = src[i] + add;
+}
+
+// n 8-byte words from device memory into pinned host memory that the device
+// maps (dst is the mapping's device-side address).  The words cross the host
+// link as the kernel's stores, not as a copy-engine transfer, so they do not
+// queue behind bulk copies to the host that are in flight on other streams.
+__global__ void k_fetch_words(unsigned long long* __restrict__ dst, const unsigned long long* __restrict__ src,
+                              int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
 // Rows into per-bin lists.  cursor[b] starts at the bin's offset; lanes that
 // hit the same bin share one atomic (warp-aggregated).
 __global__ void k_bin_scatter_symb(int64_t m, const int64_t* __restrict__ row_flp, int64_t c_ncol,

@@ -110,6 +110,9 @@ typedef struct {
 	double d2h_direct_bytes;
 	/* dense rows split across thread blocks (cas_tuning.heavy_split) */
 	int64_t split_rows;
+	/* row blocks the call computed C in (cas_tuning.out_blocks; 1 for a C
+	 * in device memory) */
+	int64_t out_blocks;
 } cas_stats;
 
 typedef struct cas_ctx cas_ctx;
@@ -162,6 +165,12 @@ typedef struct {
 	                                kinds interleaved, so they run side by side, as the reference's
 	                                high- and low-contention thread groups claim morsels from the two
 	                                ends of its cf-sorted queue (src/ams/ams_utils.c:190-216) */
+	int32_t out_blocks;          /* C returned in host memory (int32 columns) is computed in this many
+	                                row blocks of about equal A entries, each copied out while the next
+	                                is computed, into host arrays sized by sum over rows of
+	                                min(products, num_col); 0: one block under 1 GiB of C, else one per
+	                                2 GiB, at least 2 and at most 64 [0]; 1: one block, host arrays
+	                                sized by the symbolic counts; at most 64 */
 } cas_tuning;
 cas_status cas_set_tuning(cas_ctx *ctx, const cas_tuning *t);
 cas_status cas_get_tuning(const cas_ctx *ctx, cas_tuning *t);
