@@ -80,7 +80,7 @@ class CasBatchStats(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
-BATCH_MODES = {"waves": 0, "per_call": 1}
+BATCH_MODES = {"waves": 0, "per_call": 1, "concurrent": 2}
 
 
 class CasServerOpts(ctypes.Structure):

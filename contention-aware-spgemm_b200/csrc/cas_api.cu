@@ -85,6 +85,7 @@ struct cas_ctx {
   double acc_thres = 2.0;
   cudaEvent_t ev_fused[2] = {};
   cudaStream_t copy_stream = nullptr;      // copies of finished row blocks of a host C
+  std::vector<cas_ctx*> batch_workers;     // contexts of CAS_BATCH_CONCURRENT's threads
   std::string err;
   cas_stats stats{};
   int64_t launches = 0;
@@ -1712,6 +1713,8 @@ cas_status cas_create(int device, cas_ctx** out) {
 
 void cas_destroy(cas_ctx* ctx) {
   if (!ctx) return;
+  for (cas_ctx* w : ctx->batch_workers) cas_destroy(w);
+  ctx->batch_workers.clear();
   cudaSetDevice(ctx->device);
   if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
   if (ctx->copy_stream) {

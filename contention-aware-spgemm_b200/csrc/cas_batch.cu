@@ -12,7 +12,8 @@
 // bound 12 bytes * min(products, columns of the job) per row stays within
 // the budget.  A digest kernel folds each wave's rows into per-job digests,
 // subtracting each row's column shift, and the wave's C is released.
-// CAS_BATCH_PER_CALL runs one cas_spgemm per job with the same kernels.
+// CAS_BATCH_PER_CALL runs one cas_spgemm per job with the same kernels, and
+// CAS_BATCH_CONCURRENT runs them so on several host threads and streams.
 
 namespace cas {
 
@@ -427,6 +428,147 @@ cas_status batch_per_call(cas_ctx* ctx, cas_accum accum, cas_job* jobs, int64_t 
   return rc;
 }
 
+
+// CAS_BATCH_CONCURRENT: the jobs as in PER_CALL, on kBatchWorkers host
+// threads with a context each (kept by the calling context).  The threads
+// claim jobs from a shared counter, largest first by the estimate
+// nnz(A) * nnz(B) / rows(B) (longest processing time first, so the jobs
+// claimed last are short), and run them on their own streams: one job's host
+// waits overlap the others' kernels, and small jobs' kernels, which leave
+// most SMs idle, run side by side.  Digests go into the calling context's
+// per-job arrays; `ready` (recorded on its stream after they are cleared)
+// orders the workers after that, and the calling stream waits for every
+// worker's last kernel before they are read.
+constexpr int kBatchWorkers = 4;
+
+cas_status batch_concurrent(cas_ctx* ctx, cas_accum accum, cas_job* jobs, int64_t n, cas_batch_stats& st) {
+  using namespace cas;
+  const int nw = (int)std::min<int64_t>(kBatchWorkers, n);
+  cas_tuning tun;
+  cas_get_tuning(ctx, &tun);
+  while ((int)ctx->batch_workers.size() < nw) {
+    cas_ctx* w = nullptr;
+    const cas_status s = cas_create(ctx->device, &w);
+    if (s != CAS_OK) return set_err(ctx, s, "a batch worker's context could not be created");
+    ctx->batch_workers.push_back(w);
+  }
+  std::vector<int64_t> order((size_t)n);
+  std::vector<double> est((size_t)n);
+  for (int64_t j = 0; j < n; ++j) {
+    order[(size_t)j] = j;
+    const cas_csr& B = jobs[j].B;
+    est[(size_t)j] = (double)jobs[j].A.num_nnz * (double)B.num_nnz / (double)std::max<int64_t>(1, B.num_row);
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return est[(size_t)a] > est[(size_t)b]; });
+  int64_t max_rows = 0;
+  for (int64_t j = 0; j < n; ++j)
+    if (jobs[j].row_digests) max_rows = std::max(max_rows, jobs[j].A.num_row);
+  BatchOut out;
+  CAS_TRY(batch_out_alloc(ctx, n, 0, false, out));
+  cudaEvent_t ready = nullptr;
+  CAS_CUDA(ctx, cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  CAS_CUDA(ctx, cudaEventRecord(ready, ctx->stream));
+  struct Tally {
+    int64_t flop = 0, nnz = 0, runs = 0, launches = 0;
+    double h2d = 0;
+    cas_status first = CAS_OK;
+    int64_t first_job = -1;
+    std::string err;
+    cudaEvent_t done = nullptr;
+  };
+  std::vector<Tally> tally((size_t)nw);
+  std::atomic<int64_t> next{0};
+  auto work = [&](int wi) {
+    cas_ctx* w = ctx->batch_workers[(size_t)wi];
+    Tally& t = tally[(size_t)wi];
+    auto fail = [&](int64_t j, cas_status s) {
+      if (t.first == CAS_OK) {
+        t.first = s;
+        t.first_job = j;
+        t.err = w->err;
+      }
+    };
+    cudaSetDevice(w->device);
+    const int64_t l0 = w->launches;
+    int64_t* zero = nullptr;
+    uint64_t* rows = nullptr;
+    cas_status s = cas_set_tuning(w, &tun);
+    if (s == CAS_OK && cudaStreamWaitEvent(w->stream, ready, 0) != cudaSuccess)
+      s = set_err(w, CAS_ERR_CUDA, "batch worker: wait for the batch's start");
+    if (s == CAS_OK) s = dev_alloc(w, (void**)&zero, sizeof(int64_t));
+    if (s == CAS_OK && cudaMemsetAsync(zero, 0, sizeof(int64_t), w->stream) != cudaSuccess)
+      s = set_err(w, CAS_ERR_CUDA, "batch worker: memset");
+    if (s == CAS_OK && max_rows > 0) s = dev_alloc(w, (void**)&rows, sizeof(uint64_t) * (size_t)max_rows);
+    if (s != CAS_OK) fail(-1, s);
+    for (;;) {
+      const int64_t i = next.fetch_add(1);
+      if (i >= n) break;
+      const int64_t j = order[(size_t)i];
+      if (s != CAS_OK) {  // this worker cannot run jobs: the claimed one fails
+        jobs[j].status = s;
+        continue;
+      }
+      cas_csr C{};
+      C.on_device = 1;
+      cas_status js = run_spgemm(w, accum, &jobs[j].A, &jobs[j].B, &C, nullptr);
+      if (js == CAS_OK) {
+        jobs[j].flop = w->stats.flop;
+        t.flop += w->stats.flop;
+        t.nnz += C.num_nnz;
+        t.h2d += w->stats.h2d_bytes;
+        js = digest_launch(w, C, 0, nullptr, zero, zero, out.digest + j, out.nnz + j,
+                           jobs[j].row_digests ? rows : nullptr);
+        if (js == CAS_OK && jobs[j].row_digests && C.num_row > 0 &&
+            cudaMemcpyAsync(jobs[j].row_digests, rows, sizeof(uint64_t) * C.num_row, cudaMemcpyDeviceToHost,
+                            w->stream) != cudaSuccess)
+          js = set_err(w, CAS_ERR_CUDA, "row digests of job %lld", (long long)j);
+        cas_csr_free(w, &C);
+        ++t.runs;
+      }
+      jobs[j].status = js;
+      if (js != CAS_OK) fail(j, js);
+    }
+    if (zero) cudaFreeAsync(zero, w->stream);
+    if (rows) cudaFreeAsync(rows, w->stream);
+    if (cudaEventCreateWithFlags(&t.done, cudaEventDisableTiming) == cudaSuccess)
+      cudaEventRecord(t.done, w->stream);
+    t.launches = w->launches - l0;
+  };
+  std::vector<std::thread> threads;
+  for (int wi = 0; wi < nw; ++wi) threads.emplace_back(work, wi);
+  for (std::thread& th : threads) th.join();
+  cudaEventDestroy(ready);
+  cas_status first = CAS_OK;
+  for (Tally& t : tally) {
+    if (t.done) {
+      cudaStreamWaitEvent(ctx->stream, t.done, 0);
+      cudaEventDestroy(t.done);
+    }
+    st.flop += t.flop;
+    st.nnz_c += t.nnz;
+    st.h2d_bytes += t.h2d;
+    st.waves += t.runs;
+    ctx->launches += t.launches;
+    if (first == CAS_OK && t.first != CAS_OK) {
+      first = t.first;
+      set_err(ctx, t.first, "batch job %lld: %s", (long long)t.first_job, t.err.c_str());
+    }
+  }
+  std::vector<unsigned long long> hd((size_t)n), hn((size_t)n);
+  CAS_CUDA(ctx, cudaMemcpyAsync(hd.data(), out.digest, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  CAS_CUDA(ctx, cudaMemcpyAsync(hn.data(), out.nnz, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  CAS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int64_t j = 0; j < n; ++j) {
+    if (jobs[j].status != CAS_OK) continue;
+    jobs[j].digest = hd[(size_t)j];
+    jobs[j].nnz_c = (int64_t)hn[(size_t)j];
+  }
+  batch_out_free(ctx, out);
+  return first;
+}
+
 }  // namespace
 
 extern "C" {
@@ -462,7 +604,7 @@ cas_status cas_batch_run(cas_ctx* ctx, cas_accum accum, cas_job* jobs, int64_t n
   if (!ctx || (n > 0 && !jobs) || n < 0) return CAS_ERR_BAD_INPUT;
   if (accum != CAS_ACC_HASH && accum != CAS_ACC_HSERSC && accum != CAS_ACC_HYBACC)
     return set_err(ctx, CAS_ERR_BAD_INPUT, "unknown accumulator %d", (int)accum);
-  if (mode != CAS_BATCH_WAVES && mode != CAS_BATCH_PER_CALL)
+  if (mode != CAS_BATCH_WAVES && mode != CAS_BATCH_PER_CALL && mode != CAS_BATCH_CONCURRENT)
     return set_err(ctx, CAS_ERR_BAD_INPUT, "unknown batch mode %d", (int)mode);
   CAS_CUDA(ctx, cudaSetDevice(ctx->device));
   cudaGetLastError();
@@ -503,7 +645,8 @@ cas_status cas_batch_run(cas_ctx* ctx, cas_accum accum, cas_job* jobs, int64_t n
   CAS_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
   const double budget = wave_budget > 0 ? wave_budget : 32.0 * (1ull << 30);
   cas_status rc = mode == CAS_BATCH_WAVES ? batch_waves(ctx, accum, jobs, n, budget, vt == CAS_VAL_F64 ? 8 : 4, st)
-                                          : batch_per_call(ctx, accum, jobs, n, st);
+                  : mode == CAS_BATCH_PER_CALL ? batch_per_call(ctx, accum, jobs, n, st)
+                                               : batch_concurrent(ctx, accum, jobs, n, st);
   cudaEventRecord(e1, ctx->stream);
   cudaEventSynchronize(e1);
   float ms = 0;

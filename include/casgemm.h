@@ -291,7 +291,15 @@ typedef enum {
 	 * over the rows of every job in it. */
 	CAS_BATCH_WAVES = 0,
 	/* One cas_spgemm per job, in order: the same kernels, launched per job. */
-	CAS_BATCH_PER_CALL = 1
+	CAS_BATCH_PER_CALL = 1,
+	/* The jobs as in PER_CALL on 4 host threads, each with a context of its
+	 * own (created on first use and kept by the calling context): the
+	 * threads claim jobs from a shared counter, largest first by the estimate
+	 * nnz(A) * nnz(B) / rows(B), so one job's host waits overlap the others'
+	 * kernels and small jobs' kernels run side by side.  stats->seconds runs
+	 * from the batch's start on the calling context's stream to the last
+	 * worker's last kernel; kernel_launches counts the workers' launches. */
+	CAS_BATCH_CONCURRENT = 2
 } cas_batch_mode;
 
 typedef struct {

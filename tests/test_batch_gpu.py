@@ -1,8 +1,9 @@
-"""Batches of independent products (cas_batch_run) and product digests.
+"""Batches of independent products (cas_batch_run: waves, per call, concurrent workers) and product digests.
 
 Every job's digest, nnz(C), products and row digests must equal the oracle's
-for the same job run alone (its C through oracle/csr_digest), in both modes:
-the block-diagonal waves and one call per job.  Small budgets split jobs
+for the same job run alone (its C through oracle/csr_digest), in every mode:
+the block-diagonal waves, one call per job, and calls per job on several
+worker threads and streams.  Small budgets split jobs
 across waves; int32 values accumulate exactly in int64.
 """
 import numpy as np
@@ -64,7 +65,7 @@ def test_digest_matches_oracle(ctx):
     np.testing.assert_array_equal(rows, want["rows"])
 
 
-@pytest.mark.parametrize("mode", ["waves", "per_call"])
+@pytest.mark.parametrize("mode", ["waves", "per_call", "concurrent"])
 def test_batch_int_values(ctx, mode):
     jobs = small_batch(24, 7)
     out, st = ctx.batch_run(jobs, "hybacc", mode, row_digests=True)
@@ -97,7 +98,7 @@ def test_batch_general_and_empty_jobs(ctx):
     E = from_coo(40, 30, np.zeros(0, np.int64), np.zeros(0, np.int64), np.zeros(0))
     F = from_coo(30, 60, rng.integers(0, 30, 100), rng.integers(0, 60, 100), np.ones(100))
     jobs = [(G, H), (E, F), (F.transpose(), E.transpose()), (G, H)]
-    for mode in ("waves", "per_call"):
+    for mode in ("waves", "per_call", "concurrent"):
         out, _ = ctx.batch_run(jobs, "hybacc", mode)
         check(out, jobs)
 
@@ -109,3 +110,17 @@ def test_batch_rejects_bad_column(ctx):
     with pytest.raises(casgemm.CasError) as e:
         ctx.batch_run([(A, A.transpose()), (bad, A.transpose())], "hybacc", "waves")
     assert e.value.status == 1
+
+
+def test_batch_concurrent_reports_the_failing_job(ctx):
+    A = casgemm.gen_g500(6, 4, 1)
+    bad = casgemm.Csr(A.num_row, A.num_col, A.row_ptrs, A.cols.copy(), A.vals)
+    bad.cols[5] = A.num_col + 3
+    with pytest.raises(casgemm.CasError) as e:
+        ctx.batch_run([(A, A.transpose()), (bad, A.transpose()), (A, A.transpose())], "hybacc", "concurrent")
+    assert e.value.status == 1 and "job 1" in str(e.value)
+    # the context and its workers still run batches
+    jobs = small_batch(6, 3)
+    out, st = ctx.batch_run(jobs, "hybacc", "concurrent")
+    check(out, jobs)
+    assert st["jobs_ok"] == 6
