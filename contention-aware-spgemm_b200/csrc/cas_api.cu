@@ -1197,7 +1197,18 @@ cas_status prepare(cas_ctx* ctx, const cas_csr* A, const cas_csr* B, Call& c, do
                    (long long)A->num_col, (long long)B->num_row);
   if (A->val_type != B->val_type) return set_err(ctx, CAS_ERR_BAD_INPUT, "A and B have different value types");
   CAS_TRY(to_device(ctx, A, c.A, h2d));
-  CAS_TRY(to_device(ctx, B, c.B, h2d));
+  // B the same host matrix as A (C = A*A for a symmetric A, as for
+  // C = A*A^T): one device copy serves both
+  const bool alias = !A->on_device && !B->on_device && A->row_ptrs == B->row_ptrs && A->cols == B->cols &&
+                     A->rats == B->rats && A->num_row == B->num_row && A->num_col == B->num_col &&
+                     A->num_nnz == B->num_nnz && A->col_bytes == B->col_bytes;
+  if (alias) {
+    c.B.csr = c.A.csr;
+    c.B.nnz = c.A.nnz;
+    c.B.vt = c.A.vt;
+  } else {
+    CAS_TRY(to_device(ctx, B, c.B, h2d));
+  }
   c.m = A->num_row;
   c.ncol = B->num_col;
   c.vt = A->val_type;

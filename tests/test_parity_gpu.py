@@ -64,6 +64,19 @@ def test_reference_layout_int64_columns(ctx):
     check(out.csr, ref, True, "int64 columns")
 
 
+@pytest.mark.parametrize("algo", ["hash", "hybacc"])
+def test_same_host_matrix_as_both_inputs(ctx, algo):
+    """C = A*A with one host CSR passed as A and as B (a symmetric A, so A*A^T):
+    one device copy serves both, and C equals the oracle's A*A^T."""
+    A = casgemm.gen_er(12, 16, 4)
+    ref = oracle.oracle_spgemm(A, A.transpose(), algo)
+    out = ctx.spgemm(A, A, algo)
+    check(out.csr, ref, True, "A as both inputs")
+    assert out.stats["h2d_bytes"] == 8 * (A.num_row + 1) + 12 * A.nnz
+    two = ctx.spgemm(A, A.transpose(), algo)
+    assert two.stats["h2d_bytes"] == 2 * out.stats["h2d_bytes"]
+
+
 def test_runtime_phases(ctx):
     A = casgemm.gen_g500(12, 8, 9)
     out = ctx.spgemm(A, A.transpose(), "hybacc")
