@@ -618,7 +618,7 @@ def main():
     # per-kernel times for the roofline: extra steps with the bins run one at
     # a time and each bin kernel timed by CUDA events on its stream
     ctx.set_profiling(True)
-    bin_ms, bin_bytes = {}, {}
+    bin_ms, bin_bytes, bin_nnz = {}, {}, {}
     n_prof = 2
     ovf_rows, ovf_ms = 0, 0.0
     for _ in range(n_prof):
@@ -627,6 +627,7 @@ def main():
         for k, v in s["numc_bin_ms"].items():
             bin_ms[k] = bin_ms.get(k, 0.0) + v / n_prof
             bin_bytes[k] = bin_bytes.get(k, 0.0) + s["numc_bin_bytes"][k] / n_prof
+            bin_nnz[k] = s["numc_bin_nnz"][k]
         ovf_rows, ovf_ms = s["esc_overflow_rows"], ovf_ms + s["esc_overflow_ms"] / n_prof
         if s["fused_rows"]:
             bin_ms["fused"] = bin_ms.get("fused", 0.0) + s["fused_ms"] / n_prof
@@ -676,6 +677,7 @@ def main():
                      "timing": "CUDA events around the kernel, bins serialised, mean of 2 extra steps",
                      "traffic": committed_traffic(kernel_name, args.workload)},
         "numc_bins_ms": {k: round(v, 3) for k, v in bin_ms.items() if v > 0},
+        "numc_bins_nnz": {k: int(v) for k, v in bin_nnz.items() if v > 0},
         "esc_radix_fallback": {"rows": ovf_rows, "ms": round(ovf_ms, 3)},
         "pipeline_roofline": {"alg_bytes": alg_bytes_total, "frac": round(pipe_frac, 4),
                               "formula": "12*nnz(A)+12*P+12*nnz(C)+16*(m+1) over the step time"},

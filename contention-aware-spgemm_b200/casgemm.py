@@ -57,7 +57,7 @@ class CasStats(ctypes.Structure):
         ("esc_overflow_rows", ctypes.c_int64), ("esc_overflow_ms", ctypes.c_double),
         ("fused_rows", ctypes.c_int64), ("fused_flop", ctypes.c_int64), ("fused_bytes", ctypes.c_double),
         ("fused_ms", ctypes.c_double), ("d2h_direct_bytes", ctypes.c_double), ("split_rows", ctypes.c_int64),
-        ("out_blocks", ctypes.c_int64),
+        ("out_blocks", ctypes.c_int64), ("numc_bin_nnz", ctypes.c_int64 * 13),
     ]
 
 
@@ -327,7 +327,7 @@ class Context:
             "esc_overflow_rows": s.esc_overflow_rows, "esc_overflow_ms": s.esc_overflow_ms,
             "fused_rows": s.fused_rows, "fused_flop": s.fused_flop, "fused_bytes": s.fused_bytes,
             "fused_ms": s.fused_ms, "d2h_direct_bytes": s.d2h_direct_bytes, "split_rows": s.split_rows,
-            "out_blocks": s.out_blocks,
+            "out_blocks": s.out_blocks, "numc_bin_nnz": dict(zip(NUMC_BINS, list(s.numc_bin_nnz))),
         }
 
     def spgemm(self, A, B, accum: str = "hybacc", col_bytes: int = 4) -> Result:

@@ -1300,6 +1300,7 @@ cas_stats product_stats(cas_ctx* ctx, const Call& c, const DevC& o) {
     const double nzc = (double)ctx->h_counts[kSlotBinSums + kNumcBins + b];
     const double nza = (double)ctx->h_counts[kSlotBinSums + 2 * kNumcBins + b];
     s.numc_bin_flop[b] = (int64_t)ctx->h_counts[kSlotBinSums + b];
+    s.numc_bin_nnz[b] = (int64_t)nzc;
     s.numc_bin_bytes[b] = (4 + vin) * (nza + flp) + 12.0 * nzc + 16.0 * (double)c.numc_count[b];
     float ms = 0;
     if (ctx->profile && b != kNB_Zero && c.numc_count[b] > 0 &&
@@ -1347,6 +1348,7 @@ void add_stats(cas_stats& a, const cas_stats& b) {
     a.numc_bin_ms[i] += b.numc_bin_ms[i];
     a.numc_bin_bytes[i] += b.numc_bin_bytes[i];
     a.numc_bin_flop[i] += b.numc_bin_flop[i];
+    a.numc_bin_nnz[i] += b.numc_bin_nnz[i];
   }
   a.esc_overflow_rows += b.esc_overflow_rows;
   a.esc_overflow_ms += b.esc_overflow_ms;

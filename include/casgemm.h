@@ -113,6 +113,8 @@ typedef struct {
 	/* row blocks the call computed C in (cas_tuning.out_blocks; 1 for a C
 	 * in device memory) */
 	int64_t out_blocks;
+	/* nnz(C) of the rows of each numeric bin (the fused rows are not in them) */
+	int64_t numc_bin_nnz[CAS_NUMC_BINS];
 } cas_stats;
 
 typedef struct cas_ctx cas_ctx;
