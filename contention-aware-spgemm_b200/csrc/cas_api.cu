@@ -82,6 +82,8 @@ struct cas_ctx {
   int esc_max = 8192;                      // ESC rows: at most this many products
   int hash_max = 4096;                     // hash rows: at most this many distinct columns
   int out_blocks = 0;                      // C in host memory: row blocks (0: by C's size)
+  double mem_share = 1.0;                  // share of the free device memory this context sizes
+                                           // its optional scratch by (a batch worker's: 1 / workers)
   double acc_thres = 2.0;
   cudaEvent_t ev_fused[2] = {};
   cudaStream_t copy_stream = nullptr;      // copies of finished row blocks of a host C
@@ -832,7 +834,7 @@ constexpr int64_t kSplitScratch = int64_t(8) << 30;  // at most 8 GiB of slice b
 cas_status symb_split_heavy(cas_ctx* ctx, Call& c, int32_t*& rows, int64_t& n, int64_t* row_nz, cudaStream_t s) {
   using namespace cas;
   const int64_t max_slices = (c.ncol + kRankCols - 1) / kRankCols;
-  const int64_t cap = kSplitScratch / (max_slices * (kRankCols / 8));
+  const int64_t cap = (int64_t)((double)kSplitScratch * ctx->mem_share) / (max_slices * (kRankCols / 8));
   auto alloc = [&](void** p, size_t bytes) -> cas_status {
     cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, s);
     if (e != cudaSuccess) {
@@ -937,7 +939,8 @@ cas_status launch_symb_bins(cas_ctx* ctx, Call& c, int64_t* row_nz) {
           cudaGetLastError();
           free_b = 0;
         }
-        const double cap = std::max(kSavedBitmapBytes, std::min(24.0 * (1ull << 30), 0.25 * (double)free_b));
+        const double cap = ctx->mem_share *
+                           std::max(kSavedBitmapBytes, std::min(24.0 * (1ull << 30), 0.25 * (double)free_b));
         const int64_t max_slices = (c.ncol + kRankCols - 1) / kRankCols;
         c.saved_slices = (double)nd * max_slices * (kRankCols / 8) <= cap ? (int)max_slices : 1;
         if ((double)nd * c.saved_slices * (kRankCols / 8) <= cap) {
@@ -1154,7 +1157,8 @@ cas_status launch_numc_bins(cas_ctx* ctx, Call& c, const int64_t* crp, int32_t* 
         for (int k = 0; k <= kHeavyClasses - 1 - kSplitLog2; ++k) n_split += (int64_t)ctx->h_counts[kSlotHeavy + k];
         n_split = std::min(n_split, n);
         const int64_t max_slices = (c.ncol + kRankCols - 1) / kRankCols;
-        n_split = std::min<int64_t>(n_split, kSplitScratch / (max_slices * (kRankCols / 8)));
+        n_split = std::min<int64_t>(n_split,
+                                    (int64_t)((double)kSplitScratch * ctx->mem_share) / (max_slices * (kRankCols / 8)));
         if (!ctx->heavy_split) n_split = 0;
         ctx->stats.split_rows = n_split;
         if (n_split > 0) CAS_TRY(launch_heavy_split<VIn>(ctx, c, rows, n_split, crp, ccol, cval, s));
@@ -1622,6 +1626,7 @@ cas_status run_spgemm(cas_ctx* ctx, cas_accum accum, const cas_csr* A, const cas
   });
   if (st != CAS_OK) {
     free_host();
+    scratch_free(ctx, c);
     free_dev_c(o, ctx->stream);
     return finish(st);
   }

@@ -435,10 +435,13 @@ cas_status batch_per_call(cas_ctx* ctx, cas_accum accum, cas_job* jobs, int64_t 
 // nnz(A) * nnz(B) / rows(B) (longest processing time first, so the jobs
 // claimed last are short), and run them on their own streams: one job's host
 // waits overlap the others' kernels, and small jobs' kernels, which leave
-// most SMs idle, run side by side.  Digests go into the calling context's
-// per-job arrays; `ready` (recorded on its stream after they are cleared)
-// orders the workers after that, and the calling stream waits for every
-// worker's last kernel before they are read.
+// most SMs idle, run side by side.  Each worker sizes its optional scratch
+// (kept bitmaps, split rows) by 1 / kBatchWorkers of the free device memory;
+// a job that still runs out of device memory beside the others is run again
+// after them, alone, on the calling context.  Digests go into the calling
+// context's per-job arrays; `ready` (recorded on its stream after they are
+// cleared) orders the workers after that, and the calling stream waits for
+// every worker's last kernel before they are read.
 constexpr int kBatchWorkers = 4;
 
 cas_status batch_concurrent(cas_ctx* ctx, cas_accum accum, cas_job* jobs, int64_t n, cas_batch_stats& st) {
@@ -450,6 +453,7 @@ cas_status batch_concurrent(cas_ctx* ctx, cas_accum accum, cas_job* jobs, int64_
     cas_ctx* w = nullptr;
     const cas_status s = cas_create(ctx->device, &w);
     if (s != CAS_OK) return set_err(ctx, s, "a batch worker's context could not be created");
+    w->mem_share = 1.0 / kBatchWorkers;
     ctx->batch_workers.push_back(w);
   }
   std::vector<int64_t> order((size_t)n);
@@ -476,18 +480,46 @@ cas_status batch_concurrent(cas_ctx* ctx, cas_accum accum, cas_job* jobs, int64_
     std::string err;
     cudaEvent_t done = nullptr;
   };
-  std::vector<Tally> tally((size_t)nw);
+  // one job on context w: its product, and its digest into the batch's arrays
+  auto run_job = [&](cas_ctx* w, int64_t j, const int64_t* zero, uint64_t* rows, Tally& t) -> cas_status {
+    cas_csr C{};
+    C.on_device = 1;
+    cas_status js = run_spgemm(w, accum, &jobs[j].A, &jobs[j].B, &C, nullptr);
+    if (js != CAS_OK) return js;
+    jobs[j].flop = w->stats.flop;
+    t.flop += w->stats.flop;
+    t.nnz += C.num_nnz;
+    t.h2d += w->stats.h2d_bytes;
+    js = digest_launch(w, C, 0, nullptr, zero, zero, out.digest + j, out.nnz + j, jobs[j].row_digests ? rows : nullptr);
+    if (js == CAS_OK && jobs[j].row_digests && C.num_row > 0 &&
+        cudaMemcpyAsync(jobs[j].row_digests, rows, sizeof(uint64_t) * C.num_row, cudaMemcpyDeviceToHost,
+                        w->stream) != cudaSuccess)
+      js = set_err(w, CAS_ERR_CUDA, "row digests of job %lld", (long long)j);
+    cas_csr_free(w, &C);
+    ++t.runs;
+    return js;
+  };
+  // a worker's (or the calling context's) scratch for the digests
+  auto job_scratch = [&](cas_ctx* w, int64_t** zero, uint64_t** rows) -> cas_status {
+    CAS_TRY(dev_alloc(w, (void**)zero, sizeof(int64_t)));
+    CAS_CUDA(w, cudaMemsetAsync(*zero, 0, sizeof(int64_t), w->stream));
+    if (max_rows > 0) CAS_TRY(dev_alloc(w, (void**)rows, sizeof(uint64_t) * (size_t)max_rows));
+    return CAS_OK;
+  };
+  std::vector<Tally> tally((size_t)nw + 1);  // the last: the calling context's retries
   std::atomic<int64_t> next{0};
+  std::mutex retry_mu;
+  std::vector<int64_t> retry;
+  auto fail = [](Tally& t, cas_ctx* w, int64_t j, cas_status s) {
+    if (t.first == CAS_OK) {
+      t.first = s;
+      t.first_job = j;
+      t.err = w->err;
+    }
+  };
   auto work = [&](int wi) {
     cas_ctx* w = ctx->batch_workers[(size_t)wi];
     Tally& t = tally[(size_t)wi];
-    auto fail = [&](int64_t j, cas_status s) {
-      if (t.first == CAS_OK) {
-        t.first = s;
-        t.first_job = j;
-        t.err = w->err;
-      }
-    };
     cudaSetDevice(w->device);
     const int64_t l0 = w->launches;
     int64_t* zero = nullptr;
@@ -495,11 +527,8 @@ cas_status batch_concurrent(cas_ctx* ctx, cas_accum accum, cas_job* jobs, int64_
     cas_status s = cas_set_tuning(w, &tun);
     if (s == CAS_OK && cudaStreamWaitEvent(w->stream, ready, 0) != cudaSuccess)
       s = set_err(w, CAS_ERR_CUDA, "batch worker: wait for the batch's start");
-    if (s == CAS_OK) s = dev_alloc(w, (void**)&zero, sizeof(int64_t));
-    if (s == CAS_OK && cudaMemsetAsync(zero, 0, sizeof(int64_t), w->stream) != cudaSuccess)
-      s = set_err(w, CAS_ERR_CUDA, "batch worker: memset");
-    if (s == CAS_OK && max_rows > 0) s = dev_alloc(w, (void**)&rows, sizeof(uint64_t) * (size_t)max_rows);
-    if (s != CAS_OK) fail(-1, s);
+    if (s == CAS_OK) s = job_scratch(w, &zero, &rows);
+    if (s != CAS_OK) fail(t, w, -1, s);
     for (;;) {
       const int64_t i = next.fetch_add(1);
       if (i >= n) break;
@@ -508,25 +537,14 @@ cas_status batch_concurrent(cas_ctx* ctx, cas_accum accum, cas_job* jobs, int64_
         jobs[j].status = s;
         continue;
       }
-      cas_csr C{};
-      C.on_device = 1;
-      cas_status js = run_spgemm(w, accum, &jobs[j].A, &jobs[j].B, &C, nullptr);
-      if (js == CAS_OK) {
-        jobs[j].flop = w->stats.flop;
-        t.flop += w->stats.flop;
-        t.nnz += C.num_nnz;
-        t.h2d += w->stats.h2d_bytes;
-        js = digest_launch(w, C, 0, nullptr, zero, zero, out.digest + j, out.nnz + j,
-                           jobs[j].row_digests ? rows : nullptr);
-        if (js == CAS_OK && jobs[j].row_digests && C.num_row > 0 &&
-            cudaMemcpyAsync(jobs[j].row_digests, rows, sizeof(uint64_t) * C.num_row, cudaMemcpyDeviceToHost,
-                            w->stream) != cudaSuccess)
-          js = set_err(w, CAS_ERR_CUDA, "row digests of job %lld", (long long)j);
-        cas_csr_free(w, &C);
-        ++t.runs;
+      const cas_status js = run_job(w, j, zero, rows, t);
+      if (js == CAS_ERR_OOM) {  // again after the others, alone
+        std::lock_guard<std::mutex> lock(retry_mu);
+        retry.push_back(j);
+        continue;
       }
       jobs[j].status = js;
-      if (js != CAS_OK) fail(j, js);
+      if (js != CAS_OK) fail(t, w, j, js);
     }
     if (zero) cudaFreeAsync(zero, w->stream);
     if (rows) cudaFreeAsync(rows, w->stream);
@@ -538,12 +556,29 @@ cas_status batch_concurrent(cas_ctx* ctx, cas_accum accum, cas_job* jobs, int64_
   for (int wi = 0; wi < nw; ++wi) threads.emplace_back(work, wi);
   for (std::thread& th : threads) th.join();
   cudaEventDestroy(ready);
-  cas_status first = CAS_OK;
-  for (Tally& t : tally) {
+  for (int wi = 0; wi < nw; ++wi) {
+    Tally& t = tally[(size_t)wi];
     if (t.done) {
       cudaStreamWaitEvent(ctx->stream, t.done, 0);
       cudaEventDestroy(t.done);
     }
+  }
+  if (!retry.empty()) {
+    std::sort(retry.begin(), retry.end(), [&](int64_t a, int64_t b) { return est[(size_t)a] > est[(size_t)b]; });
+    Tally& t = tally[(size_t)nw];  // its launches count on the calling context itself
+    int64_t* zero = nullptr;
+    uint64_t* rows = nullptr;
+    cas_status s = job_scratch(ctx, &zero, &rows);
+    for (const int64_t j : retry) {
+      const cas_status js = s == CAS_OK ? run_job(ctx, j, zero, rows, t) : s;
+      jobs[j].status = js;
+      if (js != CAS_OK) fail(t, ctx, j, js);
+    }
+    if (zero) cudaFreeAsync(zero, ctx->stream);
+    if (rows) cudaFreeAsync(rows, ctx->stream);
+  }
+  cas_status first = CAS_OK;
+  for (Tally& t : tally) {
     st.flop += t.flop;
     st.nnz_c += t.nnz;
     st.h2d_bytes += t.h2d;

@@ -298,7 +298,10 @@ typedef enum {
 	 * own (created on first use and kept by the calling context): the
 	 * threads claim jobs from a shared counter, largest first by the estimate
 	 * nnz(A) * nnz(B) / rows(B), so one job's host waits overlap the others'
-	 * kernels and small jobs' kernels run side by side.  stats->seconds runs
+	 * kernels and small jobs' kernels run side by side.  Each worker sizes its
+	 * optional scratch by a quarter of the free device memory, and a job that
+	 * still runs out of device memory beside the others is run again after
+	 * them, alone, on the calling context.  stats->seconds runs
 	 * from the batch's start on the calling context's stream to the last
 	 * worker's last kernel; kernel_launches counts the workers' launches. */
 	CAS_BATCH_CONCURRENT = 2
