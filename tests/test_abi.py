@@ -65,3 +65,39 @@ def test_autotuner_key_is_a_function_of_the_degrees():
     assert casgemm.Autotuner.key(A, A) == casgemm.Autotuner.key(casgemm.gen_er(10, 32, 9), casgemm.gen_er(10, 32, 9))
     assert casgemm.Autotuner.key(A, A) != casgemm.Autotuner.key(G, G)
     assert casgemm.Autotuner.key(A, A).endswith("_f64")
+
+
+# every struct of include/casgemm.h that casgemm.py mirrors with ctypes
+MIRRORS = {"cas_csr": "CasCsr", "cas_runtime": "CasRuntime", "cas_stats": "CasStats", "cas_job": "CasJob",
+           "cas_batch_stats": "CasBatchStats", "cas_server_opts": "CasServerOpts", "cas_result": "CasResult",
+           "cas_server_stats": "CasServerStats", "cas_tuning": "CasTuning"}
+
+
+def test_ctypes_mirrors_match_the_header(tmp_path):
+    """Size and every field's offset of each mirrored struct, as the C compiler lays them out."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "casgemm.h"', "int main(void) {"]
+    for c_name, py_name in MIRRORS.items():
+        lines.append(f'printf("{c_name} size %zu\\n", sizeof({c_name}));')
+        for f, _ in getattr(casgemm, py_name)._fields_:
+            lines.append(f'printf("{c_name} {f} %zu\\n", offsetof({c_name}, {f}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for ln in out:
+        if ln:
+            s, f, v = ln.split()
+            got[(s, f)] = int(v)
+    for c_name, py_name in MIRRORS.items():
+        cls = getattr(casgemm, py_name)
+        assert ctypes.sizeof(cls) == got[(c_name, "size")], c_name
+        for f, _ in cls._fields_:
+            assert getattr(cls, f).offset == got[(c_name, f)], (c_name, f)
