@@ -1867,7 +1867,7 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
   // REGK: values staged in shared memory at their places and copied out in
   // order, when they fit the dead part of the arena (with the byte table
   // when the value pass walks B rows)
-  const bool seg_walk = REGK && n >= 32 * (int)(ae - as);
+  const bool seg_walk = REGK && n >= 32 * (int)(ae - as) && (int)(ae - as) >= 2 * NW;
   const size_t dead = size_t(CAP) * 6 + size_t(NB) * 2 + size_t(NCHP) * 8 + (seg_walk ? ((CAP + 15) & ~15) : 0);
   const bool stage = REGK && (size_t)nz * sizeof(AT) <= dead;
   AT* sval = reinterpret_cast<AT*>(skey);
@@ -1903,7 +1903,9 @@ k_numc_esc_idx(const int32_t* __restrict__ rows, Csr A, Csr B, int32_t b_sorted,
     __syncthreads();
   }
   // product order: a_ik * b_kj to its place (REGK: a warp per B row when
-  // the chunk's B rows average at least 32 products)
+  // the chunk's B rows average at least 32 products and there are at least
+  // two per warp; a row of a few long B rows, as in R-MAT G500 and Zipf
+  // products, would leave most warps idle that way)
   auto put = [&](VIn av, VIn bv, int p) {
     const uint16_t o = place_of[p];
     if (o == kSkip) return;
