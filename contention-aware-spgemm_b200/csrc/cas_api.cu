@@ -303,6 +303,28 @@ cas_status free_owned(cas_ctx* ctx, DevMat& m) {
   return CAS_OK;
 }
 
+// Device memory a stream-ordered allocation can still get: the device's free
+// memory plus what the pool holds reserved but unused (freed allocations it
+// keeps, since its release threshold is unbounded).  cudaMemGetInfo alone
+// would count the pool's idle reserve as taken, so sizes chosen from it would
+// shrink after every large product.
+double free_device_bytes(cas_ctx* ctx) {
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+    cudaGetLastError();
+    return 0.0;
+  }
+  double idle = 0.0;
+  cudaMemPool_t pool;
+  uint64_t reserved = 0, used = 0;  // 64-bit attribute values
+  if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess &&
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+    idle = (double)(reserved - used);
+  cudaGetLastError();
+  return (double)free_b + idle;
+}
+
 cas_status dev_alloc(cas_ctx* ctx, void** p, size_t bytes) {
   if (bytes == 0) bytes = 16;
   cudaError_t e = cudaMallocAsync(p, bytes, ctx->stream);
@@ -934,13 +956,8 @@ cas_status launch_symb_bins(cas_ctx* ctx, Call& c, int64_t* row_nz) {
         // bitmaps kept for the numeric kernel: every slice of each row when that fits a quarter
         // of the free device memory, at most 24 GiB (and at least kSavedBitmapBytes), else
         // one-slice rows only
-        size_t free_b = 0, total_b = 0;
-        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
-          cudaGetLastError();
-          free_b = 0;
-        }
-        const double cap = ctx->mem_share *
-                           std::max(kSavedBitmapBytes, std::min(24.0 * (1ull << 30), 0.25 * (double)free_b));
+        const double free_b = free_device_bytes(ctx);
+        const double cap = ctx->mem_share * std::max(kSavedBitmapBytes, std::min(24.0 * (1ull << 30), 0.25 * free_b));
         const int64_t max_slices = (c.ncol + kRankCols - 1) / kRankCols;
         c.saved_slices = (double)nd * max_slices * (kRankCols / 8) <= cap ? (int)max_slices : 1;
         if ((double)nd * c.saved_slices * (kRankCols / 8) <= cap) {
